@@ -1,0 +1,82 @@
+// bdg_dev.h -- device context shared by the CUDA translation units.
+// Not installed; the public C ABI is include/bdg/bdg_cuda.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bdg/bdg_cuda.h"
+
+#define BDGD_MAX_STAGES 12
+
+struct AxisDev {
+  int n;                    // line length
+  int nst;                  // number of Stockham stages
+  int rad[BDGD_MAX_STAGES]; // radix per stage
+  const double2 *r64;       // exp(-2 pi i m / n), m < n
+  const float2 *r32;
+};
+
+struct GeoDev {
+  int dim;
+  int cplx;   // complex (c2c) path
+  int N[3];   // N[0] = x (fastest)
+  int nxk;    // spectrum x extent: N[0]/2+1 (r2c) or N[0] (c2c)
+  int nrows;  // real-space rows along x = size / N[0]
+  long long S;  // real-space points
+  long long H;  // spectrum points per field
+  AxisDev ax[3];
+  const double *kx2[3];  // per-axis k^2 tables (N[d] entries)
+};
+
+struct FieldsDev {
+  // precision-specific copies; `w` is the wavefunction (real or interleaved complex)
+  const void *ltK, *ltM, *pK, *pM, *w;
+  const double *vdd;  // dipolar kernel (k_size doubles, spectrum layout)
+  double g_ddi;
+  double mu;
+  double inv_size;
+};
+
+struct bdgd_ctx {
+  int dim;
+  int cplx;
+  int N[3];
+  double L[3];
+  long long S, H;
+  int nxk;
+  int device;
+  cudaStream_t stream;
+  GeoDev geo;
+  // tables
+  double2 *d_roots64[3];
+  float2 *d_roots32[3];
+  double *d_kx2[3];
+  // physics (FP64 and FP32 copies)
+  double *ltK64, *ltM64, *pK64, *pM64;
+  float *ltK32, *ltM32, *pK32, *pM32;
+  void *wf64, *wf32;
+  double *vdd;
+  double g_ddi, mu;
+  int dipolar;
+  int has_wf, has_precond;
+  // scratch
+  void *spec;
+  size_t spec_bytes;
+  void *io;   // staging for host applies
+  size_t io_bytes;
+  double *gram_part;
+  size_t gram_part_bytes;
+  size_t spec_cap;  // max scratch bytes per apply chunk
+};
+
+// error helpers (defined in bdg_ops.cu)
+void bdgd_set_error(const char *fmt, ...);
+int bdgd_check(cudaError_t e, const char *what);
+int bdgd_ensure(void **ptr, size_t *have, size_t want);
+
+#define BDGD_CK(call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return bdgd_check(_e, #call); \
+  } while (0)

@@ -1,0 +1,1126 @@
+// bdg_ops.cu -- batched BdG operator applies on sm_100a.
+//
+// Every operator of the reference (pstuermer/BDG_LOBPCG) operator layer is a
+// pointwise prologue, an unnormalised 3D FFT, a k-space multiply, an inverse
+// FFT and a pointwise epilogue, applied there one column at a time through
+// FFTW (src/kinetic_impl.inc:17-30, src/matmulK_impl.inc:11-28,
+// src/matmulM_impl.inc:14-44, src/dipolar_conv_impl.inc:22-52,
+// src/precond_impl.inc:21-118).  Here one launch per FFT pass handles all
+// columns (and both halves [u; v]) of a block:
+//
+//   pass X-fwd   rows along x: prologue (p*x, conj(psi0)*x) + forward FFT
+//   pass Y-fwd   pencils along y (3D only)
+//   pass Z-fused pencils along the last axis: forward FFT, k-space multiply
+//                (k^2/2, dipolar kernel, 1/(mu + k^2/2)), inverse FFT
+//   pass Y-inv   (3D only)
+//   pass X-inv   rows: inverse FFT of every spectrum of the half + epilogue
+//                (+ localTerm*x, + 2 g psi0 * exchange, * p)
+//
+// Each pass stages its lines in shared memory and runs a mixed-radix
+// Stockham FFT (radix 8/4/2/3 butterflies in registers, generic radix for
+// other small primes).  Real fields use the r2c half spectrum (x extent
+// N/2+1) between passes, so the spectrum traffic is that of FFTW's r2c.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "bdg_dev.h"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+void bdgd_set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+int bdgd_check(cudaError_t e, const char *what) {
+  bdgd_set_error("%s: %s", what, cudaGetErrorString(e));
+  return BDGD_ERR_CUDA;
+}
+
+extern "C" const char *bdgd_last_error(void) { return g_err; }
+
+extern "C" int bdgd_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int bdgd_ensure(void **ptr, size_t *have, size_t want) {
+  if (*have >= want && *ptr) return BDGD_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *have = 0;
+  if (want == 0) return BDGD_OK;
+  BDGD_CK(cudaMalloc(ptr, want));
+  *have = want;
+  return BDGD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// complex helpers
+// ---------------------------------------------------------------------------
+template <typename T> struct Cx;
+template <> struct Cx<double> { typedef double2 t; };
+template <> struct Cx<float> { typedef float2 t; };
+
+template <typename C> __device__ __forceinline__ C cmk(double a, double b) {
+  C r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
+  C r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C csub(C a, C b) {
+  C r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) {
+  a.y = -a.y;
+  return a;
+}
+template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) {
+  a.x *= s;
+  a.y *= s;
+  return a;
+}
+// (x + i y) * (sgn * i)
+template <typename C> __device__ __forceinline__ C cmul_si(C a, int sgn) {
+  C r;
+  if (sgn > 0) {
+    r.x = -a.y;
+    r.y = a.x;
+  } else {
+    r.x = a.y;
+    r.y = -a.x;
+  }
+  return r;
+}
+
+template <typename C> __device__ __forceinline__ const C *roots_of(const AxisDev &ax);
+template <> __device__ __forceinline__ const double2 *roots_of<double2>(const AxisDev &ax) {
+  return ax.r64;
+}
+template <> __device__ __forceinline__ const float2 *roots_of<float2>(const AxisDev &ax) {
+  return ax.r32;
+}
+
+// root(m) = exp(sgn * 2 pi i m / n)
+template <typename C> __device__ __forceinline__ C rootv(const C *r, int m, int sgn) {
+  C w = __ldg(r + m);
+  if (sgn > 0) w.y = -w.y;
+  return w;
+}
+
+// ---------------------------------------------------------------------------
+// small DFT butterflies (in registers)
+// ---------------------------------------------------------------------------
+template <typename C> __device__ __forceinline__ void bfly2(C *v) {
+  C a = v[0];
+  v[0] = cadd(a, v[1]);
+  v[1] = csub(a, v[1]);
+}
+
+template <typename C> __device__ __forceinline__ void bfly4(C &v0, C &v1, C &v2, C &v3, int sgn) {
+  C a0 = cadd(v0, v2), a1 = csub(v0, v2);
+  C a2 = cadd(v1, v3), a3 = cmul_si(csub(v1, v3), sgn);
+  v0 = cadd(a0, a2);
+  v2 = csub(a0, a2);
+  v1 = cadd(a1, a3);
+  v3 = csub(a1, a3);
+}
+
+template <typename C> __device__ __forceinline__ void bfly8(C *v, int sgn) {
+  // even/odd split: E = DFT4(v0 v2 v4 v6), O = DFT4(v1 v3 v5 v7)
+  bfly4(v[0], v[2], v[4], v[6], sgn);
+  bfly4(v[1], v[3], v[5], v[7], sgn);
+  const double h = 0.70710678118654752440;
+  C o1 = v[3], o2 = v[5], o3 = v[7];
+  // o1 * exp(sgn i pi/4) = h (x - sgn y) + i h (sgn x + y)
+  C t1, t3;
+  t1.x = h * (o1.x - sgn * o1.y);
+  t1.y = h * (sgn * o1.x + o1.y);
+  C t2 = cmul_si(o2, sgn);
+  // o3 * exp(sgn i 3pi/4) = h(-x - sgn y) + i h(sgn x - y)
+  t3.x = h * (-o3.x - sgn * o3.y);
+  t3.y = h * (sgn * o3.x - o3.y);
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1];
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, t1);
+  v[5] = csub(e1, t1);
+  v[2] = cadd(e2, t2);
+  v[6] = csub(e2, t2);
+  v[3] = cadd(e3, t3);
+  v[7] = csub(e3, t3);
+}
+
+template <typename C> __device__ __forceinline__ void bfly3(C *v, int sgn) {
+  const double h = 0.86602540378443864676;
+  C t1 = cadd(v[1], v[2]);
+  C t2;
+  t2.x = v[0].x - 0.5 * t1.x;
+  t2.y = v[0].y - 0.5 * t1.y;
+  C t3 = cscale(cmul_si(csub(v[1], v[2]), sgn), h);
+  v[0] = cadd(v[0], t1);
+  v[1] = cadd(t2, t3);
+  v[2] = csub(t2, t3);
+}
+
+template <int R, typename C> struct Bfly {
+  static __device__ __forceinline__ void run(C *v, int sgn) {}
+};
+template <typename C> struct Bfly<2, C> {
+  static __device__ __forceinline__ void run(C *v, int) { bfly2(v); }
+};
+template <typename C> struct Bfly<3, C> {
+  static __device__ __forceinline__ void run(C *v, int sgn) { bfly3(v, sgn); }
+};
+template <typename C> struct Bfly<4, C> {
+  static __device__ __forceinline__ void run(C *v, int sgn) { bfly4(v[0], v[1], v[2], v[3], sgn); }
+};
+template <typename C> struct Bfly<8, C> {
+  static __device__ __forceinline__ void run(C *v, int sgn) { bfly8(v, sgn); }
+};
+
+// One Stockham stage of radix R over `nlines` lines of length n in shared
+// memory (line l at a + l*ls), a -> b.
+template <int R, typename C>
+__device__ __forceinline__ void stage_r(const C *__restrict__ a, C *__restrict__ b, int nlines,
+                                        int ls, int n, int Ns, const C *roots, int sgn) {
+  const int nb = n / R;
+  const int tot = nlines * nb;
+  const int tw = n / (Ns * R);
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int line = t / nb;
+    const int j = t - line * nb;
+    const C *src = a + line * ls;
+    C *dst = b + line * ls;
+    const int k = j % Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+    if (k) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], rootv(roots, r * k * tw, sgn));
+    }
+    Bfly<R, C>::run(v, sgn);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+  }
+}
+
+// Generic odd prime radix (5, 7, 11, 13): direct DFT with table roots.
+template <typename C>
+__device__ void stage_gen(const C *__restrict__ a, C *__restrict__ b, int nlines, int ls, int n,
+                          int Ns, int R, const C *roots, int sgn) {
+  const int nb = n / R;
+  const int tot = nlines * nb;
+  const int tw = n / (Ns * R);
+  const int wstep = n / R;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int line = t / nb;
+    const int j = t - line * nb;
+    const C *src = a + line * ls;
+    C *dst = b + line * ls;
+    const int k = j % Ns;
+    C v[16];
+    for (int r = 0; r < R; ++r) {
+      v[r] = src[j + r * nb];
+      if (k && r) v[r] = cmul(v[r], rootv(roots, r * k * tw, sgn));
+    }
+    const int base = (j / Ns) * Ns * R + k;
+    for (int q = 0; q < R; ++q) {
+      C acc = v[0];
+      for (int r = 1; r < R; ++r) acc = cadd(acc, cmul(v[r], rootv(roots, ((r * q) % R) * wstep, sgn)));
+      dst[base + q * Ns] = acc;
+    }
+  }
+}
+
+// Full FFT of `nlines` lines held in shared memory buffer a (scratch b).
+// Caller synchronises before; returns the buffer that holds the result
+// (synchronised).
+template <typename C>
+__device__ C *smem_fft(C *a, C *b, int nlines, int ls, const AxisDev &ax, int sgn) {
+  const C *roots = roots_of<C>(ax);
+  int Ns = 1;
+  for (int s = 0; s < ax.nst; ++s) {
+    const int R = ax.rad[s];
+    switch (R) {
+      case 8: stage_r<8>(a, b, nlines, ls, ax.n, Ns, roots, sgn); break;
+      case 4: stage_r<4>(a, b, nlines, ls, ax.n, Ns, roots, sgn); break;
+      case 2: stage_r<2>(a, b, nlines, ls, ax.n, Ns, roots, sgn); break;
+      case 3: stage_r<3>(a, b, nlines, ls, ax.n, Ns, roots, sgn); break;
+      default: stage_gen(a, b, nlines, ls, ax.n, Ns, R, roots, sgn); break;
+    }
+    __syncthreads();
+    C *t = a;
+    a = b;
+    b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// operator programs
+// ---------------------------------------------------------------------------
+enum { PRE_NONE = 0, PRE_PK, PRE_PM, PRE_CONJWF, PRE_DENS };
+enum { MUL_KIN = 0, MUL_DIP, MUL_PRE, MUL_ONE };
+enum { POST_RAW = 0, POST_K, POST_M, POST_TK, POST_TM, POST_DIPCONV, POST_PHI };
+
+struct Prog {
+  int nh;         // halves per column (1, or 2 for [u; v])
+  int J;          // spectra (jobs) per column
+  int nf[2];      // spectra per half
+  int j0[2];      // first job of each half
+  int pre[2][2];  // prologue per half, field
+  int mul[2][2];  // k-space multiplier per half, field
+  int post[2];    // epilogue per half
+  int jh[4], jf[4];
+};
+
+static Prog make_prog(int op, int dipolar) {
+  Prog p;
+  memset(&p, 0, sizeof p);
+  auto set_half = [&](int h, int kind) {
+    switch (kind) {
+      case BDGD_OP_KINETIC:
+        p.nf[h] = 1; p.pre[h][0] = PRE_NONE; p.mul[h][0] = MUL_KIN; p.post[h] = POST_RAW; break;
+      case BDGD_OP_K:
+        p.nf[h] = 1; p.pre[h][0] = PRE_NONE; p.mul[h][0] = MUL_KIN; p.post[h] = POST_K; break;
+      case BDGD_OP_M:
+        p.nf[h] = dipolar ? 2 : 1;
+        p.pre[h][0] = PRE_NONE; p.mul[h][0] = MUL_KIN;
+        p.pre[h][1] = PRE_CONJWF; p.mul[h][1] = MUL_DIP;
+        p.post[h] = POST_M; break;
+      case BDGD_OP_TK:
+        p.nf[h] = 1; p.pre[h][0] = PRE_PK; p.mul[h][0] = MUL_PRE; p.post[h] = POST_TK; break;
+      case BDGD_OP_TM:
+        p.nf[h] = 1; p.pre[h][0] = PRE_PM; p.mul[h][0] = MUL_PRE; p.post[h] = POST_TM; break;
+      case BDGD_OP_DIPCONV:
+        p.nf[h] = 1; p.pre[h][0] = PRE_CONJWF; p.mul[h][0] = MUL_DIP; p.post[h] = POST_DIPCONV; break;
+      case 100:  // dipolar mean field of |psi0|^2
+        p.nf[h] = 1; p.pre[h][0] = PRE_DENS; p.mul[h][0] = MUL_DIP; p.post[h] = POST_PHI; break;
+    }
+  };
+  if (op == BDGD_OP_LREP) {
+    p.nh = 2; set_half(0, BDGD_OP_K); set_half(1, BDGD_OP_M);
+  } else if (op == BDGD_OP_TLREP) {
+    p.nh = 2; set_half(0, BDGD_OP_TK); set_half(1, BDGD_OP_TM);
+  } else {
+    p.nh = 1; set_half(0, op);
+  }
+  int j = 0;
+  for (int h = 0; h < p.nh; ++h) {
+    p.j0[h] = j;
+    for (int f = 0; f < p.nf[h]; ++f) { p.jh[j] = h; p.jf[j] = f; ++j; }
+  }
+  p.J = j;
+  return p;
+}
+
+// k-space multiplier of spectrum element (ix, iy, iz), flat index kidx.
+// Same arithmetic as the reference loops: k2 = kx2[0][ix] + kx2[1][iy] +
+// kx2[2][iz]; kinetic k2 * (0.5/size) (src/kinetic_impl.inc:25-27); dipolar
+// kernel * (1/size) (src/dipolar_conv_impl.inc:41-43); preconditioner
+// (1/size) / safe_val(mu + 0.5 k2) (src/precond_impl.inc:45-48).
+__device__ __forceinline__ double kmult(const GeoDev &g, const FieldsDev &f, int kind, int ix, int iy,
+                                        int iz, long long kidx) {
+  if (kind == MUL_DIP) return __ldg(f.vdd + kidx) * f.inv_size;
+  if (kind == MUL_ONE) return 1.0;
+  double k2 = __ldg(g.kx2[0] + ix);
+  if (g.dim > 1) k2 += __ldg(g.kx2[1] + iy);
+  if (g.dim > 2) k2 += __ldg(g.kx2[2] + iz);
+  if (kind == MUL_KIN) return k2 * (0.5 * f.inv_size);
+  double d = f.mu + 0.5 * k2;
+  if (fabs(d) < 1e-8) d = 1e-8;
+  return f.inv_size / d;
+}
+
+// ---------------------------------------------------------------------------
+// element access helpers for the real (T) and complex (C) paths
+// ---------------------------------------------------------------------------
+template <typename T, bool CPLX> struct El;
+template <typename T> struct El<T, false> {
+  typedef typename Cx<T>::t C;
+  typedef T V;
+  static __device__ __forceinline__ C to_c(V v) { return cmk<C>(v, 0.0); }
+  static __device__ __forceinline__ V from_c(C c) { return c.x; }
+};
+template <typename T> struct El<T, true> {
+  typedef typename Cx<T>::t C;
+  typedef C V;
+  static __device__ __forceinline__ C to_c(V v) { return v; }
+  static __device__ __forceinline__ V from_c(C c) { return c; }
+};
+
+template <typename T, bool CPLX>
+__device__ __forceinline__ typename El<T, CPLX>::C prologue(const FieldsDev &f, int kind,
+                                                            typename El<T, CPLX>::V x, long long r) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  const T *pK = (const T *)f.pK;
+  const T *pM = (const T *)f.pM;
+  const V *w = (const V *)f.w;
+  if constexpr (CPLX) {
+    switch (kind) {
+      case PRE_PK: return cscale(x, __ldg(pK + r));
+      case PRE_PM: return cscale(x, __ldg(pM + r));
+      case PRE_CONJWF: return cmul(cconj(w[r]), x);
+      case PRE_DENS: {
+        // |psi|^2 as cabs(psi)^2 (src/dipolar_meanfield_impl.inc:33-35)
+        C z = w[r];
+        T a = hypot(z.x, z.y);
+        return cmk<C>(a * a, 0.0);
+      }
+      default: return x;
+    }
+  } else {
+    switch (kind) {
+      case PRE_PK: return cmk<C>(__ldg(pK + r) * x, 0.0);
+      case PRE_PM: return cmk<C>(__ldg(pM + r) * x, 0.0);
+      case PRE_CONJWF: return cmk<C>(w[r] * x, 0.0);
+      case PRE_DENS: {
+        T a = fabs(w[r]);
+        return cmk<C>(a * a, 0.0);
+      }
+      default: return cmk<C>(x, 0.0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pass kernels
+// ---------------------------------------------------------------------------
+// Rows along x, forward.  grid.x: row blocks, grid.y: ncol*J jobs.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) k_row_fwd(GeoDev g, Prog p, FieldsDev f, const void *__restrict__ xin,
+                                                 long long ldx, typename Cx<T>::t *__restrict__ spec, int rpb) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *a = (C *)smraw;
+  const int Nx = g.N[0];
+  C *b = a + rpb * Nx;
+  const int job = blockIdx.y;
+  const int col = job / p.J;
+  const int jj = job - col * p.J;
+  const int h = p.jh[jj], fi = p.jf[jj];
+  const int pre = p.pre[h][fi];
+  const V *src = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
+  const int row0 = blockIdx.x * rpb;
+  const int nr = min(rpb, g.nrows - row0);
+  for (int q = threadIdx.x; q < nr * Nx; q += blockDim.x) {
+    const long long r = (long long)row0 * Nx + q;
+    a[q] = prologue<T, CPLX>(f, pre, src[r], r);
+  }
+  __syncthreads();
+  C *res = smem_fft(a, b, nr, Nx, g.ax[0], -1);
+  C *dst = spec + (long long)job * g.H + (long long)row0 * g.nxk;
+  const int nxk = g.nxk;
+  for (int q = threadIdx.x; q < nr * nxk; q += blockDim.x) {
+    const int rr = q / nxk, kx = q - rr * nxk;
+    dst[q] = res[rr * Nx + kx];
+  }
+}
+
+// Pencils along y (axis 1) or z (axis 2).  mode 0 forward, 1 inverse,
+// 2 fused forward + multiply + inverse.  grid.x: kx tiles * outer, grid.y: jobs.
+template <typename T>
+__global__ void __launch_bounds__(256) k_col_pass(GeoDev g, Prog p, FieldsDev f,
+                                                  typename Cx<T>::t *__restrict__ spec, int axis, int mode,
+                                                  int tx) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int n = g.N[axis];
+  const int ld = n + 1;
+  C *a = (C *)smraw;
+  C *b = a + tx * ld;
+  const int nxk = g.nxk;
+  const int ntx = (nxk + tx - 1) / tx;
+  const int tile = blockIdx.x % ntx;
+  const int outer = blockIdx.x / ntx;
+  const int kx0 = tile * tx;
+  const int nt = min(tx, nxk - kx0);
+  long long ls, os;
+  if (axis == 1) {
+    ls = nxk;
+    os = (long long)nxk * g.N[1];
+  } else {
+    ls = (long long)nxk * g.N[1];
+    os = nxk;
+  }
+  const int job = blockIdx.y;
+  C *base = spec + (long long)job * g.H + (long long)outer * os + kx0;
+  for (int q = threadIdx.x; q < n * tx; q += blockDim.x) {
+    const int i = q / tx, t = q - i * tx;
+    if (t < nt) a[t * ld + i] = base[(long long)i * ls + t];
+  }
+  __syncthreads();
+  C *res = smem_fft(a, b, nt, ld, g.ax[axis], mode == 1 ? +1 : -1);
+  if (mode == 2) {
+    const int col = job / p.J;
+    const int jj = job - col * p.J;
+    const int kind = p.mul[p.jh[jj]][p.jf[jj]];
+    for (int q = threadIdx.x; q < n * nt; q += blockDim.x) {
+      const int t = q / n, i = q - t * n;
+      const int ix = kx0 + t;
+      int iy, iz;
+      if (axis == 1) {
+        iy = i;
+        iz = outer;
+      } else {
+        iy = outer;
+        iz = i;
+      }
+      const long long kidx = ((long long)iz * g.N[1] + iy) * nxk + ix;
+      const double m = kmult(g, f, kind, ix, iy, iz, kidx);
+      res[t * ld + i] = cscale(res[t * ld + i], (T)m);
+    }
+    __syncthreads();
+    C *other = (res == a) ? b : a;
+    res = smem_fft(res, other, nt, ld, g.ax[axis], +1);
+  }
+  for (int q = threadIdx.x; q < n * tx; q += blockDim.x) {
+    const int i = q / tx, t = q - i * tx;
+    if (t < nt) base[(long long)i * ls + t] = res[t * ld + i];
+  }
+}
+
+// Epilogue of one half at real-space point r given the inverse transforms
+// o0 (and o1 for M with dipolar exchange).  Reference arithmetic order:
+//   K: y = kin + ltK*x                      (src/matmulK_impl.inc:21-23)
+//   M: y = kin + (ltM*x + 2*(g*wf*buf))     (src/matmulM_impl.inc:30-32, dipolar_conv :49-51)
+//   T: y = out * p                          (src/precond_impl.inc:56-60)
+template <typename T, bool CPLX>
+__device__ __forceinline__ typename El<T, CPLX>::V epilogue(const FieldsDev &f, int post, int nf,
+                                                            typename El<T, CPLX>::C o0,
+                                                            typename El<T, CPLX>::C o1,
+                                                            typename El<T, CPLX>::V x, long long r) {
+  typedef typename El<T, CPLX>::V V;
+  typedef typename El<T, CPLX>::C C;
+  const T *ltK = (const T *)f.ltK;
+  const T *ltM = (const T *)f.ltM;
+  const T *pK = (const T *)f.pK;
+  const T *pM = (const T *)f.pM;
+  const V *w = (const V *)f.w;
+  const T g = (T)f.g_ddi;
+  if constexpr (CPLX) {
+    switch (post) {
+      case POST_K: return cadd(o0, cscale(x, __ldg(ltK + r)));
+      case POST_M:
+        if (nf > 1) {
+          C dc = cmul(cscale(w[r], g), o1);
+          return cadd(o0, cadd(cscale(x, __ldg(ltM + r)), cscale(dc, (T)2)));
+        }
+        return cadd(o0, cscale(x, __ldg(ltM + r)));
+      case POST_TK: return cscale(o0, __ldg(pK + r));
+      case POST_TM: return cscale(o0, __ldg(pM + r));
+      case POST_DIPCONV: return cmul(cscale(w[r], g), o0);
+      case POST_PHI: return cmk<C>(g * o0.x, 0.0);
+      default: return o0;
+    }
+  } else {
+    const T y0 = o0.x;
+    switch (post) {
+      case POST_K: return y0 + __ldg(ltK + r) * x;
+      case POST_M:
+        if (nf > 1) {
+          const T dc = (g * w[r]) * o1.x;
+          return y0 + (__ldg(ltM + r) * x + (T)2 * dc);
+        }
+        return y0 + __ldg(ltM + r) * x;
+      case POST_TK: return y0 * __ldg(pK + r);
+      case POST_TM: return y0 * __ldg(pM + r);
+      case POST_DIPCONV: return (g * w[r]) * o0.x;
+      case POST_PHI: return g * o0.x;
+      default: return y0;
+    }
+  }
+}
+
+// Rows along x, inverse + epilogue.  grid.x: row blocks, grid.y: ncol*nh units.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) k_row_inv(GeoDev g, Prog p, FieldsDev f,
+                                                 const typename Cx<T>::t *__restrict__ spec,
+                                                 const void *__restrict__ xin, long long ldx, void *__restrict__ yout,
+                                                 long long ldy, int rpb) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int Nx = g.N[0];
+  const int nxk = g.nxk;
+  const int unit = blockIdx.y;
+  const int col = unit / p.nh;
+  const int h = unit - col * p.nh;
+  const int nf = p.nf[h];
+  const int row0 = blockIdx.x * rpb;
+  const int nr = min(rpb, g.nrows - row0);
+  C *buf = (C *)smraw;
+  C *res[2] = {nullptr, nullptr};
+  for (int fi = 0; fi < nf; ++fi) {
+    C *a = buf + (2 * fi) * rpb * Nx;
+    C *b = a + rpb * Nx;
+    const C *src = spec + ((long long)col * p.J + p.j0[h] + fi) * g.H + (long long)row0 * nxk;
+    for (int q = threadIdx.x; q < nr * Nx; q += blockDim.x) {
+      const int rr = q / Nx, kx = q - rr * Nx;
+      C v;
+      if (CPLX || kx < nxk) {
+        v = src[rr * nxk + kx];
+      } else {
+        v = cconj(src[rr * nxk + (Nx - kx)]);
+      }
+      a[q] = v;
+    }
+    __syncthreads();
+    res[fi] = smem_fft(a, b, nr, Nx, g.ax[0], +1);
+  }
+  const V *xs = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
+  V *ys = (V *)yout + (long long)col * ldy + (long long)h * g.S;
+  const int post = p.post[h];
+  for (int q = threadIdx.x; q < nr * Nx; q += blockDim.x) {
+    const long long r = (long long)row0 * Nx + q;
+    C o0 = res[0][q];
+    C o1 = (nf > 1) ? res[1][q] : o0;
+    V xv = (post == POST_K || post == POST_M) ? xs[r] : V();
+    ys[r] = epilogue<T, CPLX>(f, post, nf, o0, o1, xv, r);
+  }
+}
+
+// 1D problems: one kernel does prologue, forward, multiply, inverse and
+// epilogue per row.  grid.y: units.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) k_row_fused1d(GeoDev g, Prog p, FieldsDev f, const void *__restrict__ xin,
+                                                     long long ldx, void *__restrict__ yout, long long ldy) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int Nx = g.N[0];
+  const int unit = blockIdx.y;
+  const int col = unit / p.nh;
+  const int h = unit - col * p.nh;
+  const int nf = p.nf[h];
+  C *buf = (C *)smraw;
+  C *res[2] = {nullptr, nullptr};
+  const V *xs = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
+  V *ys = (V *)yout + (long long)col * ldy + (long long)h * g.S;
+  for (int fi = 0; fi < nf; ++fi) {
+    C *a = buf + (2 * fi) * Nx;
+    C *b = a + Nx;
+    const int pre = p.pre[h][fi];
+    for (int q = threadIdx.x; q < Nx; q += blockDim.x) a[q] = prologue<T, CPLX>(f, pre, xs[q], q);
+    __syncthreads();
+    C *r = smem_fft(a, b, 1, Nx, g.ax[0], -1);
+    const int kind = p.mul[h][fi];
+    for (int q = threadIdx.x; q < Nx; q += blockDim.x) {
+      // full-length spectrum: kx2 is defined on all N entries (wrapped k)
+      const int kk = (CPLX || q < g.nxk) ? q : (Nx - q);
+      const double m = kmult(g, f, kind, q, 0, 0, kk);
+      r[q] = cscale(r[q], (T)m);
+    }
+    __syncthreads();
+    C *o = (r == a) ? b : a;
+    res[fi] = smem_fft(r, o, 1, Nx, g.ax[0], +1);
+  }
+  const int post = p.post[h];
+  for (int q = threadIdx.x; q < Nx; q += blockDim.x) {
+    C o0 = res[0][q];
+    C o1 = (nf > 1) ? res[1][q] : o0;
+    V xv = (post == POST_K || post == POST_M) ? xs[q] : V();
+    ys[q] = epilogue<T, CPLX>(f, post, nf, o0, o1, xv, q);
+  }
+}
+
+// Swap: y = [x_v; x_u] (src/matmulSwap_impl.inc:18-22), copied in words of W.
+template <typename W>
+__global__ void k_swap(const unsigned char *__restrict__ x, long long ldxb, unsigned char *__restrict__ y,
+                       long long ldyb, long long halfb) {
+  const long long nw = halfb / (long long)sizeof(W);
+  const long long col = blockIdx.y;
+  const W *xs = (const W *)(x + col * ldxb);
+  W *ys = (W *)(y + col * ldyb);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw;
+       i += (long long)gridDim.x * blockDim.x) {
+    ys[i] = xs[nw + i];
+    ys[nw + i] = xs[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side: context
+// ---------------------------------------------------------------------------
+static int factorize(int n, int *rad) {
+  int k = 0;
+  if (n == 1) return 0;
+  while (n % 8 == 0 && n > 8 && k < BDGD_MAX_STAGES) { rad[k++] = 8; n /= 8; }
+  while (n % 4 == 0 && k < BDGD_MAX_STAGES) { rad[k++] = 4; n /= 4; }
+  while (n % 2 == 0 && k < BDGD_MAX_STAGES) { rad[k++] = 2; n /= 2; }
+  while (n % 8 == 0 && k < BDGD_MAX_STAGES) { rad[k++] = 8; n /= 8; }
+  const int primes[] = {3, 5, 7, 11, 13};
+  for (int pi = 0; pi < 5; ++pi)
+    while (n % primes[pi] == 0 && k < BDGD_MAX_STAGES) { rad[k++] = primes[pi]; n /= primes[pi]; }
+  if (n != 1) return -1;
+  return k;
+}
+
+// Stage order: radix 8 first (largest butterflies on the Ns = 1 stage).
+static int plan_axis(int n, int *rad) {
+  int tmp[BDGD_MAX_STAGES];
+  int k = factorize(n, tmp);
+  if (k < 0) return -1;
+  // pull 8s together: factorize returns 8s only when n has 16 | n; recombine 4*2 -> 8
+  int c8 = 0, c4 = 0, c2 = 0, cnt = 0;
+  int others[BDGD_MAX_STAGES];
+  int no = 0;
+  for (int i = 0; i < k; ++i) {
+    if (tmp[i] == 8) c8++;
+    else if (tmp[i] == 4) c4++;
+    else if (tmp[i] == 2) c2++;
+    else others[no++] = tmp[i];
+  }
+  int p2 = 3 * c8 + 2 * c4 + c2;  // power of two exponent
+  while (p2 >= 3) { rad[cnt++] = 8; p2 -= 3; }
+  if (p2 == 2) rad[cnt++] = 4;
+  if (p2 == 1) rad[cnt++] = 2;
+  for (int i = 0; i < no; ++i) rad[cnt++] = others[i];
+  return cnt;
+}
+
+extern "C" int bdgd_create(bdgd_ctx **out, uint64_t dim, const uint64_t *N, const double *L,
+                           int complex_psi0) {
+  *out = nullptr;
+  if (dim < 1 || dim > 3) {
+    bdgd_set_error("bdgd_create: dim must be 1, 2 or 3");
+    return BDGD_ERR_ARG;
+  }
+  bdgd_ctx *c = (bdgd_ctx *)calloc(1, sizeof(bdgd_ctx));
+  if (!c) return BDGD_ERR_ARG;
+  c->dim = (int)dim;
+  c->cplx = complex_psi0 ? 1 : 0;
+  for (int d = 0; d < 3; ++d) {
+    c->N[d] = d < (int)dim ? (int)N[d] : 1;
+    c->L[d] = d < (int)dim ? L[d] : 1.0;
+  }
+  c->S = (long long)c->N[0] * c->N[1] * c->N[2];
+  c->nxk = c->cplx ? c->N[0] : c->N[0] / 2 + 1;
+  c->H = (long long)c->nxk * c->N[1] * c->N[2];
+  c->spec_cap = (size_t)4 << 30;
+  if (const char *e = getenv("BDG_SPEC_CAP_MB")) c->spec_cap = (size_t)atoll(e) << 20;
+  if (cudaGetDevice(&c->device) != cudaSuccess) {
+    cudaGetLastError();
+    free(c);
+    bdgd_set_error("bdgd_create: no CUDA device");
+    return BDGD_ERR_CUDA;
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    free(c);
+    return bdgd_check(e, "cudaStreamCreateWithFlags");
+  }
+  GeoDev &g = c->geo;
+  memset(&g, 0, sizeof g);
+  g.dim = c->dim;
+  g.cplx = c->cplx;
+  for (int d = 0; d < 3; ++d) g.N[d] = c->N[d];
+  g.nxk = c->nxk;
+  g.nrows = (int)(c->S / c->N[0]);
+  g.S = c->S;
+  g.H = c->H;
+  for (int d = 0; d < 3; ++d) {
+    const int n = c->N[d];
+    int nst = plan_axis(n, g.ax[d].rad);
+    if (nst < 0) {
+      bdgd_set_error("bdgd_create: N[%d] = %d has a prime factor above 13", d, n);
+      bdgd_destroy(&c);
+      return BDGD_ERR_UNSUPPORTED;
+    }
+    g.ax[d].n = n;
+    g.ax[d].nst = nst;
+    double2 *h64 = (double2 *)malloc(sizeof(double2) * n);
+    float2 *h32 = (float2 *)malloc(sizeof(float2) * n);
+    double *hk = (double *)malloc(sizeof(double) * n);
+    const long double tau = 6.283185307179586476925286766559L;
+    for (int m = 0; m < n; ++m) {
+      // exp(-2 pi i m/n), reduced to the first octant's symmetric angle for accuracy
+      long double ang = tau * (long double)m / (long double)n;
+      h64[m].x = (double)cosl(ang);
+      h64[m].y = (double)-sinl(ang);
+      h32[m].x = (float)h64[m].x;
+      h32[m].y = (float)h64[m].y;
+      // k_j^2 as the reference builds kx2 (src/matmul_ctx.c:103-113)
+      const double dk = 2.0 * M_PI / c->L[d];
+      const double kj = (m <= n / 2) ? (dk * (double)m) : (dk * (double)(m - n));
+      hk[m] = kj * kj;
+    }
+    cudaError_t e1 = cudaMalloc(&c->d_roots64[d], sizeof(double2) * n);
+    cudaError_t e2 = cudaMalloc(&c->d_roots32[d], sizeof(float2) * n);
+    cudaError_t e3 = cudaMalloc(&c->d_kx2[d], sizeof(double) * n);
+    if (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) {
+      cudaMemcpy(c->d_roots64[d], h64, sizeof(double2) * n, cudaMemcpyHostToDevice);
+      cudaMemcpy(c->d_roots32[d], h32, sizeof(float2) * n, cudaMemcpyHostToDevice);
+      cudaMemcpy(c->d_kx2[d], hk, sizeof(double) * n, cudaMemcpyHostToDevice);
+    }
+    free(h64);
+    free(h32);
+    free(hk);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+      bdgd_destroy(&c);
+      return bdgd_check(cudaErrorMemoryAllocation, "cudaMalloc(tables)");
+    }
+    g.ax[d].r64 = c->d_roots64[d];
+    g.ax[d].r32 = c->d_roots32[d];
+    g.kx2[d] = c->d_kx2[d];
+  }
+  *out = c;
+  return BDGD_OK;
+}
+
+extern "C" void bdgd_destroy(bdgd_ctx **pc) {
+  if (!pc || !*pc) return;
+  bdgd_ctx *c = *pc;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int d = 0; d < 3; ++d) {
+    cudaFree(c->d_roots64[d]);
+    cudaFree(c->d_roots32[d]);
+    cudaFree(c->d_kx2[d]);
+  }
+  void *bufs[] = {c->ltK64, c->ltM64, c->pK64, c->pM64, c->ltK32, c->ltM32, c->pK32,
+                  c->pM32,  c->wf64,  c->wf32, c->vdd,  c->spec,  c->io,    c->gram_part};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  free(c);
+  *pc = nullptr;
+}
+
+extern "C" void *bdgd_stream(bdgd_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+extern "C" int bdgd_synchronize(bdgd_ctx *c) {
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  return BDGD_OK;
+}
+
+// upload a host double array and its float copy
+static int upload_pair(bdgd_ctx *c, double **d64, float **d32, const double *h, long long n) {
+  if (!*d64) BDGD_CK(cudaMalloc((void **)d64, sizeof(double) * n));
+  if (!*d32) BDGD_CK(cudaMalloc((void **)d32, sizeof(float) * n));
+  BDGD_CK(cudaMemcpyAsync(*d64, h, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  float *tmp = (float *)malloc(sizeof(float) * n);
+  for (long long i = 0; i < n; ++i) tmp[i] = (float)h[i];
+  cudaError_t e = cudaMemcpyAsync(*d32, tmp, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream);
+  cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  free(tmp);
+  if (e != cudaSuccess) return bdgd_check(e, "upload");
+  if (e2 != cudaSuccess) return bdgd_check(e2, "upload sync");
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_set_local_terms(bdgd_ctx *c, const double *ltK, const double *ltM) {
+  int rc;
+  if (ltK && (rc = upload_pair(c, &c->ltK64, &c->ltK32, ltK, c->S))) return rc;
+  if (ltM && (rc = upload_pair(c, &c->ltM64, &c->ltM32, ltM, c->S))) return rc;
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_set_precond(bdgd_ctx *c, const double *sK, const double *sM, double mu) {
+  int rc;
+  if (sK && (rc = upload_pair(c, &c->pK64, &c->pK32, sK, c->S))) return rc;
+  if (sM && (rc = upload_pair(c, &c->pM64, &c->pM32, sM, c->S))) return rc;
+  c->mu = mu;
+  c->has_precond = (sK && sM) ? 1 : c->has_precond;
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_set_wavefunction(bdgd_ctx *c, const void *wf) {
+  if (!wf) return BDGD_OK;
+  const long long n = c->S * (c->cplx ? 2 : 1);
+  double *d64 = (double *)c->wf64;
+  float *d32 = (float *)c->wf32;
+  int rc = upload_pair(c, &d64, &d32, (const double *)wf, n);
+  c->wf64 = d64;
+  c->wf32 = d32;
+  if (rc) return rc;
+  c->has_wf = 1;
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_set_dipolar(bdgd_ctx *c, const double *vdd, double g_ddi, int enabled) {
+  c->g_ddi = g_ddi;
+  c->dipolar = enabled && c->dim == 3;
+  if (vdd) {
+    if (!c->vdd) BDGD_CK(cudaMalloc((void **)&c->vdd, sizeof(double) * c->H));
+    BDGD_CK(cudaMemcpyAsync(c->vdd, vdd, sizeof(double) * c->H, cudaMemcpyHostToDevice, c->stream));
+    BDGD_CK(cudaStreamSynchronize(c->stream));
+  }
+  return BDGD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host side: apply
+// ---------------------------------------------------------------------------
+static const int kThreads = 256;
+
+static int rows_per_block(int Nx) {
+  int r = 1024 / Nx;
+  return r < 1 ? 1 : r;
+}
+
+template <typename T, bool CPLX>
+static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx, void *y, long long ldy,
+                       int ncol, int only_fwd, int only_bwd) {
+  typedef typename Cx<T>::t C;
+  const bool f32 = sizeof(T) == 4;
+  FieldsDev fd;
+  fd.ltK = f32 ? (const void *)c->ltK32 : (const void *)c->ltK64;
+  fd.ltM = f32 ? (const void *)c->ltM32 : (const void *)c->ltM64;
+  fd.pK = f32 ? (const void *)c->pK32 : (const void *)c->pK64;
+  fd.pM = f32 ? (const void *)c->pM32 : (const void *)c->pM64;
+  fd.w = f32 ? c->wf32 : c->wf64;
+  fd.vdd = c->vdd;
+  fd.g_ddi = c->g_ddi;
+  fd.mu = c->mu;
+  fd.inv_size = 1.0 / (double)c->S;
+  const GeoDev &g = c->geo;
+  const int Nx = c->N[0];
+  const int rpb = rows_per_block(Nx);
+  const int nrb = (g.nrows + rpb - 1) / rpb;
+  if (c->dim == 1 && !only_fwd && !only_bwd) {
+    int maxnf = p.nf[0] > p.nf[p.nh - 1] ? p.nf[0] : p.nf[p.nh - 1];
+    size_t sm = sizeof(C) * 2 * maxnf * Nx;
+    if (sm > 48 * 1024)
+      BDGD_CK(cudaFuncSetAttribute(k_row_fused1d<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid(1, ncol * p.nh);
+    k_row_fused1d<T, CPLX><<<grid, kThreads, sm, c->stream>>>(g, p, fd, x, ldx, y, ldy);
+    BDGD_CK(cudaGetLastError());
+    return BDGD_OK;
+  }
+  // column chunking bounded by the scratch cap
+  const size_t per_col = sizeof(C) * (size_t)p.J * (size_t)g.H;
+  int chunk = ncol;
+  if (per_col * (size_t)chunk > c->spec_cap) {
+    chunk = (int)(c->spec_cap / per_col);
+    if (chunk < 1) chunk = 1;
+  }
+  if (only_fwd || only_bwd) chunk = ncol;  // raw transforms use the whole scratch as I/O
+  int rc = bdgd_ensure(&c->spec, &c->spec_bytes, per_col * (size_t)chunk);
+  if (rc) return rc;
+  C *spec = (C *)c->spec;
+  const int tx = f32 ? 16 : 8;
+  for (int c0 = 0; c0 < ncol; c0 += chunk) {
+    const int nc = (ncol - c0) < chunk ? (ncol - c0) : chunk;
+    const size_t esz = CPLX ? sizeof(C) : sizeof(T);
+    const void *xc = (const char *)x + (size_t)c0 * ldx * esz;
+    void *yc = (char *)y + (size_t)c0 * ldy * esz;
+    if (!only_bwd) {
+      size_t sm = sizeof(C) * 2 * rpb * Nx;
+      if (sm > 48 * 1024)
+        BDGD_CK(cudaFuncSetAttribute(k_row_fwd<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_row_fwd<T, CPLX><<<dim3(nrb, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, xc, ldx, spec, rpb);
+      BDGD_CK(cudaGetLastError());
+    }
+    // middle / last axes
+    for (int ax = 1; ax < c->dim && !only_bwd; ++ax) {
+      const int last = (ax == c->dim - 1);
+      const int mode = (last && !only_fwd) ? 2 : 0;
+      const int n = c->N[ax];
+      const int ntx = (c->nxk + tx - 1) / tx;
+      const int outer = (ax == 1) ? c->N[2] : c->N[1];
+      size_t sm = sizeof(C) * 2 * tx * (n + 1);
+      if (sm > 48 * 1024)
+        BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, mode, tx);
+      BDGD_CK(cudaGetLastError());
+    }
+    if (only_fwd) break;
+    const int first_inv = only_bwd ? c->dim - 1 : c->dim - 2;
+    for (int ax = first_inv; ax >= 1; --ax) {
+      const int n = c->N[ax];
+      const int ntx = (c->nxk + tx - 1) / tx;
+      const int outer = (ax == 1) ? c->N[2] : c->N[1];
+      size_t sm = sizeof(C) * 2 * tx * (n + 1);
+      if (sm > 48 * 1024)
+        BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, 1, tx);
+      BDGD_CK(cudaGetLastError());
+    }
+    {
+      int maxnf = 1;
+      for (int h = 0; h < p.nh; ++h) maxnf = p.nf[h] > maxnf ? p.nf[h] : maxnf;
+      size_t sm = sizeof(C) * 2 * maxnf * rpb * Nx;
+      if (sm > 48 * 1024)
+        BDGD_CK(cudaFuncSetAttribute(k_row_inv<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_row_inv<T, CPLX><<<dim3(nrb, nc * p.nh), kThreads, sm, c->stream>>>(g, p, fd, spec, xc, ldx, yc, ldy, rpb);
+      BDGD_CK(cudaGetLastError());
+    }
+  }
+  return BDGD_OK;
+}
+
+static int check_ready(bdgd_ctx *c, int op) {
+  const bool needs_lt = op == BDGD_OP_K || op == BDGD_OP_M || op == BDGD_OP_LREP;
+  const bool needs_p = op == BDGD_OP_TK || op == BDGD_OP_TM || op == BDGD_OP_TLREP;
+  const bool needs_wf = op == BDGD_OP_DIPCONV || ((op == BDGD_OP_M || op == BDGD_OP_LREP) && c->dipolar);
+  if (needs_lt && (!c->ltK64 || !c->ltM64)) {
+    bdgd_set_error("operator needs localTermK/localTermM");
+    return BDGD_ERR_STATE;
+  }
+  if (needs_p && (!c->pK64 || !c->pM64)) {
+    bdgd_set_error("preconditioner needs precond_sqrtK/M (bdg_set_mu)");
+    return BDGD_ERR_STATE;
+  }
+  if (needs_wf && !c->wf64) {
+    bdgd_set_error("operator needs the wavefunction");
+    return BDGD_ERR_STATE;
+  }
+  if ((op == BDGD_OP_DIPCONV || (c->dipolar && (op == BDGD_OP_M || op == BDGD_OP_LREP))) && !c->vdd) {
+    bdgd_set_error("dipolar operator needs the dipolar kernel");
+    return BDGD_ERR_STATE;
+  }
+  return BDGD_OK;
+}
+
+static int dispatch(bdgd_ctx *c, const Prog &p, int prec, const void *x, long long ldx, void *y, long long ldy,
+                    int ncol, int only_fwd, int only_bwd) {
+  if (prec == BDGD_F32) {
+    if (c->cplx) return run_program<float, true>(c, p, x, ldx, y, ldy, ncol, only_fwd, only_bwd);
+    return run_program<float, false>(c, p, x, ldx, y, ldy, ncol, only_fwd, only_bwd);
+  }
+  if (c->cplx) return run_program<double, true>(c, p, x, ldx, y, ldy, ncol, only_fwd, only_bwd);
+  return run_program<double, false>(c, p, x, ldx, y, ldy, ncol, only_fwd, only_bwd);
+}
+
+extern "C" int bdgd_apply(bdgd_ctx *c, int op, int prec, const void *d_x, uint64_t ldx, void *d_y, uint64_t ldy,
+                          uint64_t ncol) {
+  if (!c || !d_x || !d_y) {
+    bdgd_set_error("bdgd_apply: null argument");
+    return BDGD_ERR_ARG;
+  }
+  if (ncol == 0) return BDGD_OK;
+  if (op < 0 || op > BDGD_OP_DIPCONV) {
+    bdgd_set_error("bdgd_apply: unknown operator %d", op);
+    return BDGD_ERR_ARG;
+  }
+  const size_t esz = (prec == BDGD_F32 ? 4 : 8) * (c->cplx ? 2 : 1);
+  if (op == BDGD_OP_SWAP) {
+    const long long halfb = c->S * (long long)esz;
+    const long long ldxb = (long long)ldx * esz, ldyb = (long long)ldy * esz;
+    const uintptr_t al = (uintptr_t)d_x | (uintptr_t)d_y | (uintptr_t)halfb | (uintptr_t)ldxb | (uintptr_t)ldyb;
+    const int wsz = (al % 16 == 0) ? 16 : (al % 8 == 0) ? 8 : 4;
+    long long blocks = (halfb / wsz + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    dim3 grid((unsigned)blocks, (unsigned)ncol);
+    const unsigned char *xb = (const unsigned char *)d_x;
+    unsigned char *yb = (unsigned char *)d_y;
+    if (wsz == 16) k_swap<uint4><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
+    else if (wsz == 8) k_swap<unsigned long long><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
+    else k_swap<unsigned int><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
+    BDGD_CK(cudaGetLastError());
+    return BDGD_OK;
+  }
+  int rc = check_ready(c, op);
+  if (rc) return rc;
+  if (op == BDGD_OP_DIPCONV && c->dim != 3) {
+    bdgd_set_error("dipolar convolution requires dim == 3");
+    return BDGD_ERR_ARG;
+  }
+  Prog p = make_prog(op, c->dipolar && c->dim == 3);
+  return dispatch(c, p, prec, d_x, (long long)ldx, d_y, (long long)ldy, (int)ncol, 0, 0);
+}
+
+extern "C" int bdgd_apply_host(bdgd_ctx *c, int op, const void *x, void *y, uint64_t ncol) {
+  const int two = (op == BDGD_OP_LREP || op == BDGD_OP_TLREP || op == BDGD_OP_SWAP) ? 2 : 1;
+  const size_t esz = c->cplx ? 16 : 8;
+  const size_t colb = (size_t)c->S * two * esz;
+  int rc = bdgd_ensure(&c->io, &c->io_bytes, 2 * colb * ncol);
+  if (rc) return rc;
+  char *dx = (char *)c->io;
+  char *dy = dx + colb * ncol;
+  BDGD_CK(cudaMemcpyAsync(dx, x, colb * ncol, cudaMemcpyHostToDevice, c->stream));
+  rc = bdgd_apply(c, op, BDGD_F64, dx, (uint64_t)c->S * two, dy, (uint64_t)c->S * two, ncol);
+  if (rc) return rc;
+  BDGD_CK(cudaMemcpyAsync(y, dy, colb * ncol, cudaMemcpyDeviceToHost, c->stream));
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_dipolar_meanfield(bdgd_ctx *c, double *phi_out) {
+  if (!c->wf64 || !c->vdd) {
+    bdgd_set_error("dipolar mean field needs wavefunction and kernel");
+    return BDGD_ERR_STATE;
+  }
+  Prog p = make_prog(100, 0);
+  const size_t esz = c->cplx ? 16 : 8;
+  int rc = bdgd_ensure(&c->io, &c->io_bytes, 2 * esz * c->S);
+  if (rc) return rc;
+  char *dx = (char *)c->io;
+  char *dy = dx + esz * c->S;
+  BDGD_CK(cudaMemsetAsync(dx, 0, esz * c->S, c->stream));
+  rc = dispatch(c, p, BDGD_F64, dx, c->S, dy, c->S, 1, 0, 0);
+  if (rc) return rc;
+  if (c->cplx) {
+    BDGD_CK(cudaMemcpy2DAsync(phi_out, sizeof(double), dy, 2 * sizeof(double), sizeof(double), c->S,
+                              cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    BDGD_CK(cudaMemcpyAsync(phi_out, dy, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  }
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_fft_host(bdgd_ctx *c, int forward, const void *in, void *out, uint64_t ncol) {
+  Prog p = make_prog(BDGD_OP_KINETIC, 0);
+  p.post[0] = POST_RAW;
+  p.mul[0][0] = MUL_ONE;
+  const size_t esz = c->cplx ? 16 : 8;
+  const size_t rb = esz * (size_t)c->S * ncol;
+  const size_t kb = 16 * (size_t)c->H * ncol;
+  int rc = bdgd_ensure(&c->io, &c->io_bytes, rb);
+  if (rc) return rc;
+  rc = bdgd_ensure(&c->spec, &c->spec_bytes, kb);
+  if (rc) return rc;
+  if (forward) {
+    BDGD_CK(cudaMemcpyAsync(c->io, in, rb, cudaMemcpyHostToDevice, c->stream));
+    rc = dispatch(c, p, BDGD_F64, c->io, c->S, c->io, c->S, (int)ncol, 1, 0);
+    if (rc) return rc;
+    if (c->dim == 1) {
+      // 1D: the row pass wrote the spectrum already
+    }
+    BDGD_CK(cudaMemcpyAsync(out, c->spec, kb, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    BDGD_CK(cudaMemcpyAsync(c->spec, in, kb, cudaMemcpyHostToDevice, c->stream));
+    rc = dispatch(c, p, BDGD_F64, c->io, c->S, c->io, c->S, (int)ncol, 0, 1);
+    if (rc) return rc;
+    BDGD_CK(cudaMemcpyAsync(out, c->io, rb, cudaMemcpyDeviceToHost, c->stream));
+  }
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  return BDGD_OK;
+}

@@ -1,0 +1,74 @@
+/*
+ * bdg_b200.h -- options and statistics of the B200 library that have no
+ * counterpart in the reference API (pstuermer/BDG_LOBPCG include/bdg/bdg.h).
+ * All default to the reference's behaviour, so code that never calls them
+ * gets the reference semantics.
+ */
+#ifndef BDG_B200_H
+#define BDG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bdg_t bdg_t;
+
+/* Operator/preconditioner arithmetic inside the solver. */
+enum {
+  BDG_PREC_F64 = 0,  /* everything FP64 (default) */
+  BDG_PREC_MIXED = 1 /* FP32 operator + preconditioner applies and FP32
+                        blocks; FP64 Gram accumulation, small dense work,
+                        final residual check and FP64 refinement */
+};
+
+/* Meaning of the solver tolerance `tol`.  The reference delegates it to an
+ * external library whose definition is not available. */
+enum {
+  BDG_CONV_BACKWARD = 0,     /* ||A x - w B x|| / ((||A||_est + |w|) ||x||) <= tol
+                                for each of the nev wanted pairs (default) */
+  BDG_CONV_TRUE_RESIDUAL = 1 /* ||K M v - w^2 v|| / ||v|| <= tol */
+};
+
+typedef struct {
+  uint64_t iterations;     /* iLOBPCG iterations of the last solve */
+  uint64_t refine_iterations;
+  double seconds_total;    /* wall time of bdg_solve (upload to download) */
+  double seconds_device;   /* device time of the iteration loop (CUDA events) */
+  double ms_apply_A;       /* accumulated device ms per stage */
+  double ms_apply_T;
+  double ms_residual;
+  double ms_gram;
+  double ms_small_dense;
+  double ms_update;
+  uint64_t cols_apply_A;   /* columns pushed through A and T */
+  uint64_t cols_apply_T;
+  double max_residual;     /* final convergence measure over the nev pairs */
+  double max_true_residual;/* final ||KMv - w^2 v||/||v|| over the nev pairs */
+  int status;              /* 0 ok, <0 CUDA / numerical failure */
+} bdg_solve_stats_t;
+
+void bdg_set_precision(bdg_t *bdg, int precision);
+void bdg_set_convergence(bdg_t *bdg, int criterion);
+/* Restrict the search to the B-orthogonal complement of the Goldstone
+ * Jordan chain {[psi0; 0], [0; M^-1 psi0]} (real psi0 only), so the nev
+ * wanted pairs are the lowest nonzero modes. */
+void bdg_set_goldstone_deflation(bdg_t *bdg, int enable);
+/* FP64 iterations appended to a BDG_PREC_MIXED solve (default 3 max). */
+void bdg_set_refinement(bdg_t *bdg, int max_iters);
+const bdg_solve_stats_t *bdg_solve_stats(const bdg_t *bdg);
+/* bdg_set_trap with the potential already evaluated on the grid
+ * (V[size], x fastest, at r_i = (i - N/2) L / N); same state rules. */
+void bdg_set_trap_grid(bdg_t *bdg, const double *V);
+/* bdg_set_local_interactions with U_K(|psi_i|^2) and U_M(|psi_i|^2) already
+ * evaluated per grid point; same state rules and accumulation. */
+void bdg_set_local_interactions_grid(bdg_t *bdg, const double *uK, const double *uM);
+/* Full solver block after a solve: n x sizeSub column-major (host), or NULL. */
+const void *bdg_solver_block(const bdg_t *bdg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDG_B200_H */

@@ -1,0 +1,110 @@
+/*
+ * bdg_cuda.h -- the thin C ABI between the host C library and the sm_100a
+ * kernels.  Plain pointers and sizes only.  Device pointers are expected
+ * where a name says `d_`; all device work is ordered on the context's own
+ * CUDA stream (bdgd_stream).
+ *
+ * These entry points replace, as block (many-column) device calls, the
+ * reference's single-column host operators of pstuermer/BDG_LOBPCG:
+ *   BDGD_OP_KINETIC  kinetic_{d,z}      src/kinetic_impl.inc:17-30
+ *   BDGD_OP_K        matmulK_{d,z}      src/matmulK_impl.inc:11-28
+ *   BDGD_OP_M        matmulM_{d,z}      src/matmulM_impl.inc:14-44
+ *   BDGD_OP_LREP     matmulLrep_{d,z}   src/matmulLrep_impl.inc:13-18
+ *   BDGD_OP_SWAP     matmulSwap_{d,z}   src/matmulSwap_impl.inc:14-26
+ *   BDGD_OP_TK/TM    precondK/M_{d,z}   src/precond_impl.inc:21-111
+ *   BDGD_OP_TLREP    precondLrep_{d,z}  src/precond_impl.inc:113-118
+ *   BDGD_OP_DIPCONV  dipolar_conv_{d,z} src/dipolar_conv_impl.inc:22-52
+ * and the dense Gram work of the external iLOBPCG (call site
+ * src/solver.c:262).
+ */
+#ifndef BDG_CUDA_H
+#define BDG_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bdgd_ctx bdgd_ctx;
+
+enum {
+  BDGD_OP_KINETIC = 0,
+  BDGD_OP_K = 1,
+  BDGD_OP_M = 2,
+  BDGD_OP_LREP = 3,
+  BDGD_OP_SWAP = 4,
+  BDGD_OP_TK = 5,
+  BDGD_OP_TM = 6,
+  BDGD_OP_TLREP = 7,
+  BDGD_OP_DIPCONV = 8
+};
+
+enum { BDGD_F64 = 0, BDGD_F32 = 1 };
+
+enum {
+  BDGD_OK = 0,
+  BDGD_ERR_CUDA = -1,
+  BDGD_ERR_ARG = -2,
+  BDGD_ERR_UNSUPPORTED = -3,
+  BDGD_ERR_STATE = -4
+};
+
+/* Message of the last failing call of this thread. */
+const char *bdgd_last_error(void);
+/* Number of visible CUDA devices (0 without a GPU); never fails. */
+int bdgd_device_count(void);
+
+/* Grid N[0..dim-1] (x fastest), box L; complex_psi0 selects c2c transforms. */
+int bdgd_create(bdgd_ctx **out, uint64_t dim, const uint64_t *N, const double *L,
+                int complex_psi0);
+void bdgd_destroy(bdgd_ctx **ctx);
+void *bdgd_stream(bdgd_ctx *ctx);
+int bdgd_synchronize(bdgd_ctx *ctx);
+
+/* Physics arrays from host memory (size doubles each; wf is size f64 or size
+ * interleaved (re, im) pairs on the complex path; vdd has k_size doubles in
+ * the spectrum layout).  NULL leaves an array unchanged. */
+int bdgd_set_local_terms(bdgd_ctx *ctx, const double *ltK, const double *ltM);
+int bdgd_set_wavefunction(bdgd_ctx *ctx, const void *wf);
+int bdgd_set_precond(bdgd_ctx *ctx, const double *sqrtK, const double *sqrtM,
+                     double mu);
+int bdgd_set_dipolar(bdgd_ctx *ctx, const double *vdd, double g_ddi, int enabled);
+
+/* y = op(x) for ncol columns of device memory.  Column j of x starts at
+ * x + j*ldx elements (f64, c64 or, with prec = BDGD_F32, f32 / c32).
+ * LREP/TLREP/SWAP columns are [u; v] of 2*size elements, the others size
+ * elements.  x and y must not overlap. */
+int bdgd_apply(bdgd_ctx *ctx, int op, int prec, const void *d_x, uint64_t ldx,
+               void *d_y, uint64_t ldy, uint64_t ncol);
+
+/* Same as bdgd_apply on host memory (copies in, applies, copies out). */
+int bdgd_apply_host(bdgd_ctx *ctx, int op, const void *x, void *y, uint64_t ncol);
+
+/* Dipolar mean field phi = g_ddi * F^-1[vdd/size F(|wf|^2)] (real part) of
+ * the uploaded wavefunction and kernel, written to host phi_out[size]. */
+int bdgd_dipolar_meanfield(bdgd_ctx *ctx, double *phi_out);
+
+/* Unnormalised forward/backward transform of ncol host fields, for plan
+ * round-trip checks: forward maps size reals (or complex) to k_size complex
+ * values in the FFTW r2c (or c2c) layout, backward the reverse. */
+int bdgd_fft_host(bdgd_ctx *ctx, int forward, const void *in, void *out,
+                  uint64_t ncol);
+
+/* ---- Gram contraction of the iLOBPCG Rayleigh-Ritz step ----------------
+ * For a block S (n x k, column-major, leading dimension lds, n = 2*half)
+ * and AS (n x k, leading dimension ldas), writes four k x k column-major
+ * FP64 matrices to d_out (leading dimension k, consecutive):
+ *   Guu = S_u^H S_u, Gvv = S_v^H S_v, Guv = S_u^H S_v, Ga = S^H AS
+ * where S_u are rows [0, half) and S_v rows [half, n).  With B = swap,
+ * S^H S = Guu + Gvv and S^H B S = Guv + Guv^H.  Accumulation is FP64
+ * (DMMA); prec selects FP64 or FP32 inputs; cplx selects complex data. */
+int bdgd_gram(bdgd_ctx *ctx, int prec, int cplx, uint64_t half, uint64_t k,
+              const void *d_S, uint64_t lds, const void *d_AS, uint64_t ldas,
+              double *d_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDG_CUDA_H */

@@ -1,0 +1,91 @@
+"""The CPU oracle against the reference's own known answers (pins the
+oracle), plus oracle self-consistency.  No GPU."""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+from oracle import bdg_oracle as O
+
+
+@pytest.mark.parametrize("case", cases.CASES, ids=lambda f: f.__name__)
+def test_known_answer_oracle(case):
+    cases.check(case(cases.OracleAdapter))
+
+
+def _uniform_1d(cplx):
+    ctx = O.Ctx(1, [64], [2 * math.pi], cplx)
+    O.set_system(ctx)
+    O.set_wavefunction(ctx, np.ones(64))
+    O.set_local_interactions(ctx, lambda n: n, lambda n: n)
+    O.set_mu(ctx, 1.0)
+    return ctx
+
+
+def test_oracle_solver_1d_uniform():
+    """tests/test_bdg_1d_uniform.c:60-140 restated on the oracle solver:
+    two eigenvalues at sqrt(1.25), at least one at sqrt(8), within 1%."""
+    ctx = _uniform_1d(False)
+    X0 = O.gaussian_block_bpositive(ctx, 10, 0)
+    r = O.ilobpcg(ctx, X0, 4, 200, 1e-4)
+    assert r.converged >= 4
+    ev = r.eigvals[:4]
+    E1, E2 = math.sqrt(1.25), math.sqrt(8.0)
+    assert np.sum(np.abs(ev - E1) < 0.01 * E1) == 2
+    assert np.sum(np.abs(ev - E2) < 0.01 * E2) >= 1
+
+
+def test_oracle_solver_d_vs_z():
+    """tests/test_bdg_1d_uniform.c:142-230: complex path matches real path."""
+    rd = O.ilobpcg(_uniform_1d(False), O.gaussian_block_bpositive(_uniform_1d(False), 10, 0), 4, 200, 1e-4)
+    cz = _uniform_1d(True)
+    rz = O.ilobpcg(cz, O.gaussian_block_bpositive(cz, 10, 0), 4, 200, 1e-4)
+    E1 = math.sqrt(1.25)
+    d1 = rd.eigvals[np.argmin(np.abs(rd.eigvals - E1))]
+    z1 = rz.eigvals[np.argmin(np.abs(rz.eigvals - E1))]
+    assert abs(d1 - z1) < 1e-4
+
+
+def test_rr_pencil_properties():
+    """C^T (S^T B S) C = I and C^T (S^T A S) C = diag(lam) on a random
+    definite pencil."""
+    rng = np.random.default_rng(0)
+    S = 50
+    K = rng.standard_normal((S, S)); K = K @ K.T + S * np.eye(S)
+    M = rng.standard_normal((S, S)); M = M @ M.T + S * np.eye(S)
+    Xu = rng.standard_normal((6, S))
+    X = np.concatenate([Xu, Xu + 0.1 * rng.standard_normal((6, S))], axis=1)
+    AX = np.concatenate([X[:, :S] @ K, X[:, S:] @ M], axis=1)
+    Guu = X[:, :S] @ X[:, :S].T
+    Gvv = X[:, S:] @ X[:, S:].T
+    Guv = X[:, :S] @ X[:, S:].T
+    Ga = X @ AX.T
+    lam, C = O.rr_pencil(Guu, Gvv, Guv, Ga, 3)
+    Gb = Guv + Guv.T
+    assert np.allclose(C.T @ Gb @ C, np.eye(3), atol=1e-10)
+    assert np.allclose(C.T @ Ga @ C, np.diag(lam), atol=1e-8 * np.max(np.abs(lam)))
+    assert np.all(np.diff(lam) >= 0)
+
+
+def test_oracle_dense_known_answer_1d():
+    """Solver eigenvalues vs a dense eig(K M) of the same 1D trapped problem."""
+    N, L = 48, 12.0
+    ctx = O.Ctx(1, [N], [L])
+    O.set_system(ctx)
+    x = (np.arange(N) - N / 2) * L / N
+    psi = np.exp(-x * x / 2)
+    psi /= math.sqrt(np.sum(psi ** 2) * L / N)
+    O.set_trap_array(ctx, 0.5 * x * x)
+    O.set_wavefunction(ctx, psi)
+    O.set_local_interactions(ctx, lambda n: 0.0 * n, lambda n: 0.0 * n)
+    O.set_mu(ctx, 0.5)
+    E = np.eye(N)
+    Kd = O.matmulK(ctx, E).T
+    Md = O.matmulM(ctx, E).T
+    w2 = np.sort(np.linalg.eigvals(Kd @ Md).real)
+    omega = np.sqrt(np.clip(w2, 0, None))
+    X0 = O.gaussian_block_bpositive(ctx, 8, 3)
+    r = O.ilobpcg(ctx, X0, 4, 300, 1e-10)
+    assert r.converged >= 4
+    assert np.allclose(r.eigvals[1:4], omega[1:4], rtol=1e-7)
