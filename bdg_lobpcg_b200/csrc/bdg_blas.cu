@@ -20,28 +20,30 @@
 #include "bdg_blas.h"
 
 // ---------------------------------------------------------------------------
-// Gram contraction
+// Gram contraction: a list of tasks C_t = A_t^H B_t (tall-skinny, FP64 acc.)
 // ---------------------------------------------------------------------------
 #define GT 64    // output tile (GT x GT)
 #define GRK 32   // contraction rows per shared-memory stage
 #define GLD (GRK + 4)
+#define GMAXT 48
 
-struct GramProb {
-  const void *a;   // A base (element (r, i) at a[(i*lda + r)*es + comp])
-  const void *b;
-  long long lda, ldb;
-  long long rows;  // contraction length
-  int comp_a, comp_b;
+struct GTask {
+  const void *a, *b;
+  long long lda, ldb;  // leading dimensions in elements
+  long long rows;
+  int ka, kb, out, i0, j0, sym, mirror;
+  int ta, tb;          // tiles along a, b
+  int tile0;           // first global tile of this task
+  long long part0;     // offset of this task's partials (doubles)
 };
 
-struct GramArgs {
-  GramProb pr[20];
-  int nprob;
-  int k;
-  int es;          // 1 real, 2 complex (interleaved)
+struct GArgs {
+  GTask t[GMAXT];
+  int nt;
+  int ntiles;
   int nsplit;
-  long long chunk; // rows per split (multiple of GRK)
-  double *part;    // [nprob][nsplit][k][k]
+  long long chunk;
+  double *part;
 };
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
@@ -50,60 +52,103 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <typename T>
-__device__ __forceinline__ void stage_tile(double *sm, const T *__restrict__ base, long long ld, int es, int comp,
-                                           int c0, int k, long long r0, long long rend) {
-  // sm[c][r], c < GT, r < GRK; column c of the operand is contiguous along r
+// stage a GT x GRK tile: sm[c][r] (component comp of column c0+c, rows r0..)
+template <typename T, int ES>
+__device__ __forceinline__ void stage_tile(double *sm, const T *__restrict__ base, long long ld, int comp, int c0,
+                                           int kc, long long r0, long long rend) {
   for (int q = threadIdx.x; q < GT * GRK; q += blockDim.x) {
     const int c = q / GRK, r = q - c * GRK;
     const long long rr = r0 + r;
     double v = 0.0;
-    if (c0 + c < k && rr < rend) v = (double)base[((long long)(c0 + c) * ld + rr) * es + comp];
+    if (c0 + c < kc && rr < rend) v = (double)base[((long long)(c0 + c) * ld + rr) * ES + comp];
     sm[c * GLD + r] = v;
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(128) k_gram(GramArgs g) {
-  __shared__ __align__(16) double sA[GT * GLD];
-  __shared__ __align__(16) double sB[GT * GLD];
-  const int ntile = (g.k + GT - 1) / GT;
-  const int ti = blockIdx.x % ntile, tj = blockIdx.x / ntile;
-  const int split = blockIdx.y, p = blockIdx.z;
-  const GramProb pr = g.pr[p];
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) k_gram_tasks(GArgs g) {
+  extern __shared__ __align__(16) double gsm[];
+  double *sAr = gsm, *sBr = gsm + GT * GLD;
+  double *sAi = gsm + 2 * GT * GLD, *sBi = gsm + 3 * GT * GLD;
+  // locate task and tile
+  int t = 0;
+  while (t + 1 < g.nt && (int)blockIdx.x >= g.t[t + 1].tile0) ++t;
+  const GTask tk = g.t[t];
+  int local = blockIdx.x - tk.tile0, ti, tj;
+  if (tk.sym) {  // upper-triangular tiles ti <= tj, row by row
+    ti = 0;
+    int rowlen = tk.tb;
+    while (local >= rowlen) {
+      local -= rowlen;
+      ++ti;
+      rowlen = tk.tb - ti;
+    }
+    tj = ti + local;
+  } else {
+    ti = local / tk.tb;
+    tj = local - ti * tk.tb;
+  }
+  const int split = blockIdx.y;
   const long long rbeg = (long long)split * g.chunk;
   long long rend = rbeg + g.chunk;
-  if (rend > pr.rows) rend = pr.rows;
+  if (rend > tk.rows) rend = tk.rows;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wi = warp & 1, wj = warp >> 1;  // 2 x 2 warps, 32 x 32 each
-  double acc[4][4][2];
+  const int wi = warp & 1, wj = warp >> 1;
+  const int lr = lane & 3, lc = lane >> 2;
+  double acc[4][4][2], aci[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  const T *A = (const T *)pr.a;
-  const T *B = (const T *)pr.b;
-  const int lr = lane & 3, lc = lane >> 2;
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b][0] = acc[a][b][1] = 0.0;
+      aci[a][b][0] = aci[a][b][1] = 0.0;
+    }
+  const T *A = (const T *)tk.a;
+  const T *B = (const T *)tk.b;
+  constexpr int ES = CPLX ? 2 : 1;
   for (long long r0 = rbeg; r0 < rend; r0 += GRK) {
-    stage_tile<T>(sA, A, pr.lda, g.es, pr.comp_a, ti * GT, g.k, r0, rend);
-    stage_tile<T>(sB, B, pr.ldb, g.es, pr.comp_b, tj * GT, g.k, r0, rend);
+    stage_tile<T, ES>(sAr, A, tk.lda, 0, ti * GT, tk.ka, r0, rend);
+    stage_tile<T, ES>(sBr, B, tk.ldb, 0, tj * GT, tk.kb, r0, rend);
+    if (CPLX) {
+      stage_tile<T, ES>(sAi, A, tk.lda, 1, ti * GT, tk.ka, r0, rend);
+      stage_tile<T, ES>(sBi, B, tk.ldb, 1, tj * GT, tk.kb, r0, rend);
+    }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < GRK; kk += 4) {
-      double af[4], bf[4];
+      double ar[4], br[4];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) af[mi] = sA[(wi * 32 + mi * 8 + lc) * GLD + kk + lr];
+      for (int mi = 0; mi < 4; ++mi) ar[mi] = sAr[(wi * 32 + mi * 8 + lc) * GLD + kk + lr];
 #pragma unroll
-      for (int nj = 0; nj < 4; ++nj) bf[nj] = sB[(wj * 32 + nj * 8 + lc) * GLD + kk + lr];
+      for (int nj = 0; nj < 4; ++nj) br[nj] = sBr[(wj * 32 + nj * 8 + lc) * GLD + kk + lr];
 #pragma unroll
       for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-        for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], af[mi], bf[nj]);
+        for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+      if (CPLX) {
+        // conj(A)^T B: re += Ar Br + Ai Bi ; im += Ar Bi - Ai Br
+        double ai[4], bi[4], nai[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+          ai[mi] = sAi[(wi * 32 + mi * 8 + lc) * GLD + kk + lr];
+          nai[mi] = -ai[mi];
+        }
+#pragma unroll
+        for (int nj = 0; nj < 4; ++nj) bi[nj] = sBi[(wj * 32 + nj * 8 + lc) * GLD + kk + lr];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj) {
+            dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], ar[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], nai[mi], br[nj]);
+          }
+      }
     }
     __syncthreads();
   }
-  // D fragment: row = lane >> 2, cols 2*(lane & 3) + {0, 1}
-  double *out = g.part + ((long long)p * g.nsplit + split) * (long long)g.k * g.k;
+  // D fragment: row = lane >> 2, cols 2*(lane & 3) + {0, 1}; partials [split][kb][ka] (col-major)
+  double *out = g.part + tk.part0 + (long long)split * tk.ka * tk.kb * ES;
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -112,125 +157,154 @@ __global__ void __launch_bounds__(128) k_gram(GramArgs g) {
       for (int e = 0; e < 2; ++e) {
         const int i = ti * GT + wi * 32 + mi * 8 + lc;
         const int j = tj * GT + wj * 32 + nj * 8 + 2 * lr + e;
-        if (i < g.k && j < g.k) out[(long long)j * g.k + i] = acc[mi][nj][e];  // column-major
+        if (i < tk.ka && j < tk.kb) {
+          const long long o = ((long long)j * tk.ka + i) * ES;
+          out[o] = acc[mi][nj][e];
+          if (CPLX) out[o + 1] = aci[mi][nj][e];
+        }
       }
 }
 
-// out[b] (k x k, column-major, real or interleaved complex) =
-//   sum over terms t of block b/component c: sign * sum_split part[prob]
-struct GramReduce {
-  int nterm[8];        // per (block, comp) slot: block*2 + comp
-  int prob[8][4];
-  double sign[8][4];
-  int nblk, cplx, k, nsplit;
-};
-
-__global__ void k_gram_reduce(GramReduce R, const double *__restrict__ part, double *__restrict__ out) {
-  const long long kk = (long long)R.k * R.k;
-  const int ncomp = R.cplx ? 2 : 1;
-  const long long total = kk * R.nblk * ncomp;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const long long e = q % kk;
-    const long long bc = q / kk;  // block*ncomp + comp
-    const int blk = (int)(bc / ncomp), comp = (int)(bc % ncomp);
-    const int slot = blk * 2 + comp;
-    double s = 0.0;
-    for (int t = 0; t < R.nterm[slot]; ++t) {
-      const double *pp = part + (long long)R.prob[slot][t] * R.nsplit * kk + e;
-      double a = 0.0;
-      for (int sp = 0; sp < R.nsplit; ++sp) a += pp[(long long)sp * kk];
-      s += R.sign[slot][t] * a;
-    }
-    if (R.cplx)
-      out[(blk * kk + e) * 2 + comp] = s;
-    else
-      out[blk * kk + e] = s;
-  }
-}
-
-extern "C" int bdgd_gram(bdgd_ctx *c, int prec, int cplx, uint64_t half, uint64_t k, const void *d_S, uint64_t lds,
-                         const void *d_AS, uint64_t ldas, double *d_out) {
-  if (k == 0) return BDGD_OK;
+// Sum the split partials of every task into its output block (and its
+// mirror); sym tasks read the lower triangle from the computed upper tiles.
+__global__ void k_gram_tasks_reduce(GArgs g, int cplx, int ldo, double *__restrict__ outbuf) {
   const int es = cplx ? 2 : 1;
-  const size_t esz = (prec == BDGD_F32 ? 4 : 8);
-  GramArgs g;
-  memset(&g, 0, sizeof g);
-  g.k = (int)k;
-  g.es = es;
-  GramReduce R;
-  memset(&R, 0, sizeof R);
-  R.nblk = 4;
-  R.cplx = cplx;
-  R.k = (int)k;
-  // real contractions over rows [0, half): (A, B) pairs per output block
-  //   0 Guu = Su^T Su   1 Gvv = Sv^T Sv   2 Guv = Su^T Sv   3 Ga = Su^T ASu + Sv^T ASv
-  const char *S = (const char *)d_S;
-  const char *AS = (const char *)d_AS;
-  const char *Su = S, *Sv = S + half * es * esz;
-  const char *Au = AS, *Av = AS + half * es * esz;
-  struct Pair { const char *a, *b; long long la, lb; int blk; };
-  Pair pairs[5] = {{Su, Su, (long long)lds, (long long)lds, 0},
-                   {Sv, Sv, (long long)lds, (long long)lds, 1},
-                   {Su, Sv, (long long)lds, (long long)lds, 2},
-                   {Su, Au, (long long)lds, (long long)ldas, 3},
-                   {Sv, Av, (long long)lds, (long long)ldas, 3}};
-  int np = 0;
-  for (int pi = 0; pi < 5; ++pi) {
-    if (!cplx) {
-      GramProb &q = g.pr[np];
-      q.a = pairs[pi].a; q.b = pairs[pi].b; q.lda = pairs[pi].la; q.ldb = pairs[pi].lb;
-      q.rows = (long long)half; q.comp_a = q.comp_b = 0;
-      const int slot = pairs[pi].blk * 2;
-      R.prob[slot][R.nterm[slot]] = np;
-      R.sign[slot][R.nterm[slot]++] = 1.0;
-      ++np;
-    } else {
-      // (Ar - i Ai)^T (Br + i Bi): re = Ar Br + Ai Bi, im = Ar Bi - Ai Br
-      const int ca[4] = {0, 1, 0, 1}, cb[4] = {0, 1, 1, 0};
-      const int comp[4] = {0, 0, 1, 1};
-      const double sg[4] = {1.0, 1.0, 1.0, -1.0};
-      for (int t = 0; t < 4; ++t) {
-        GramProb &q = g.pr[np];
-        q.a = pairs[pi].a; q.b = pairs[pi].b; q.lda = pairs[pi].la; q.ldb = pairs[pi].lb;
-        q.rows = (long long)half; q.comp_a = ca[t]; q.comp_b = cb[t];
-        const int slot = pairs[pi].blk * 2 + comp[t];
-        R.prob[slot][R.nterm[slot]] = np;
-        R.sign[slot][R.nterm[slot]++] = sg[t];
-        ++np;
-      }
+  const int t = blockIdx.y;
+  const GTask tk = g.t[t];
+  const long long kk = (long long)tk.ka * tk.kb;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < kk; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % tk.ka), j = (int)(q / tk.ka);
+    bool conj = false;
+    int si = i, sj = j;
+    if (tk.sym && (i / GT) > (j / GT)) {  // lower tile: take the transpose element
+      si = j;
+      sj = i;
+      conj = true;
+    }
+    double re = 0.0, im = 0.0;
+    const double *pp = g.part + tk.part0 + ((long long)sj * tk.ka + si) * es;
+    for (int sp = 0; sp < g.nsplit; ++sp) {
+      re += pp[(long long)sp * kk * es];
+      if (cplx) im += pp[(long long)sp * kk * es + 1];
+    }
+    if (conj) im = -im;
+    double *o = outbuf + (long long)tk.out * ldo * ldo * es;
+    const long long dst = ((long long)(tk.j0 + j) * ldo + tk.i0 + i) * es;
+    o[dst] = re;
+    if (cplx) o[dst + 1] = im;
+    if (tk.mirror) {
+      const long long mdst = ((long long)(tk.i0 + i) * ldo + tk.j0 + j) * es;
+      o[mdst] = re;
+      if (cplx) o[mdst + 1] = -im;
     }
   }
-  g.nprob = np;
-  const int ntile = (int)((k + GT - 1) / GT);
-  const int ctas_per_split = ntile * ntile * np;
-  int nsplit = (4 * 148 + ctas_per_split - 1) / ctas_per_split;
-  const long long maxsplit = ((long long)half + 4 * GRK - 1) / (4 * GRK);
+}
+
+extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
+                               double *d_out) {
+  if (ntask <= 0) return BDGD_OK;
+  if (ntask > GMAXT) {
+    bdgd_set_error("bdgd_gram_tasks: at most %d tasks", GMAXT);
+    return BDGD_ERR_ARG;
+  }
+  const int es = cplx ? 2 : 1;
+  GArgs g;
+  memset(&g, 0, sizeof g);
+  g.nt = ntask;
+  long long maxrows = 0;
+  int tiles = 0;
+  for (int i = 0; i < ntask; ++i) {
+    GTask &t = g.t[i];
+    const bdgd_gram_task &s = tasks[i];
+    t.a = s.a;
+    t.b = s.b;
+    t.lda = (long long)s.lda;
+    t.ldb = (long long)s.ldb;
+    t.rows = (long long)s.rows;
+    t.ka = s.ka;
+    t.kb = s.kb;
+    t.out = s.out;
+    t.i0 = s.i0;
+    t.j0 = s.j0;
+    t.sym = s.sym && s.ka == s.kb;
+    t.mirror = s.mirror;
+    t.ta = (s.ka + GT - 1) / GT;
+    t.tb = (s.kb + GT - 1) / GT;
+    t.tile0 = tiles;
+    tiles += t.sym ? t.ta * (t.ta + 1) / 2 : t.ta * t.tb;
+    if (t.rows > maxrows) maxrows = t.rows;
+  }
+  g.ntiles = tiles;
+  int nsplit = (4 * 148 + tiles - 1) / tiles;
+  const long long maxsplit = (maxrows + 8 * GRK - 1) / (8 * GRK);
   if (nsplit > maxsplit) nsplit = (int)maxsplit;
   if (nsplit < 1) nsplit = 1;
-  long long chunk = ((long long)half + nsplit - 1) / nsplit;
+  long long chunk = (maxrows + nsplit - 1) / nsplit;
   chunk = (chunk + GRK - 1) / GRK * GRK;
-  nsplit = (int)(((long long)half + chunk - 1) / chunk);
+  if (chunk < GRK) chunk = GRK;
+  nsplit = (int)((maxrows + chunk - 1) / chunk);
+  if (nsplit < 1) nsplit = 1;
   g.nsplit = nsplit;
   g.chunk = chunk;
-  R.nsplit = nsplit;
-  int rc = bdgd_ensure((void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * np * nsplit * k * k);
+  long long off = 0;
+  for (int i = 0; i < ntask; ++i) {
+    g.t[i].part0 = off;
+    off += (long long)nsplit * g.t[i].ka * g.t[i].kb * es;
+  }
+  int rc = bdgd_ensure((void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
   if (rc) return rc;
   g.part = c->gram_part;
-  dim3 grid(ntile * ntile, nsplit, np);
-  if (prec == BDGD_F32)
-    k_gram<float><<<grid, 128, 0, c->stream>>>(g);
-  else
-    k_gram<double><<<grid, 128, 0, c->stream>>>(g);
+  // tasks with fewer rows than nsplit*chunk simply see empty splits (zeros)
+  const size_t sm = sizeof(double) * GT * GLD * (cplx ? 4 : 2);
+  dim3 grid(tiles, nsplit);
+  if (prec == BDGD_F32) {
+    if (cplx) {
+      BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_gram_tasks<float, true><<<grid, 128, sm, c->stream>>>(g);
+    } else {
+      k_gram_tasks<float, false><<<grid, 128, sm, c->stream>>>(g);
+    }
+  } else {
+    if (cplx) {
+      BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_gram_tasks<double, true><<<grid, 128, sm, c->stream>>>(g);
+    } else {
+      k_gram_tasks<double, false><<<grid, 128, sm, c->stream>>>(g);
+    }
+  }
   BDGD_CK(cudaGetLastError());
-  const long long tot = (long long)k * k * 4 * (cplx ? 2 : 1);
-  int nb = (int)((tot + 255) / 256);
-  if (nb > 2048) nb = 2048;
-  k_gram_reduce<<<nb, 256, 0, c->stream>>>(R, c->gram_part, d_out);
+  k_gram_tasks_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, cplx, ldo, d_out);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
 
+// The four Rayleigh-Ritz blocks of one contiguous block S (kept for direct
+// checks of the contraction): Guu, Gvv, Guv, Ga.
+extern "C" int bdgd_gram(bdgd_ctx *c, int prec, int cplx, uint64_t half, uint64_t k, const void *d_S, uint64_t lds,
+                         const void *d_AS, uint64_t ldas, double *d_out) {
+  if (k == 0) return BDGD_OK;
+  const size_t esz = (size_t)(prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
+  const char *S = (const char *)d_S, *AS = (const char *)d_AS;
+  bdgd_gram_task t[5];
+  memset(t, 0, sizeof t);
+  const void *as[5] = {S, S + half * esz, S, S, S + half * esz};
+  const void *bs[5] = {S, S + half * esz, S + half * esz, AS, AS + half * esz};
+  const int outs[5] = {0, 1, 2, 3, 4};
+  for (int i = 0; i < 5; ++i) {
+    t[i].a = as[i];
+    t[i].b = bs[i];
+    t[i].lda = lds;
+    t[i].ldb = (i >= 3) ? ldas : lds;
+    t[i].rows = half;
+    t[i].ka = t[i].kb = (int)k;
+    t[i].out = outs[i];
+    t[i].sym = (i < 2);
+  }
+  // Ga = Su^H ASu + Sv^H ASv: contract over all n rows in one task instead
+  t[3].rows = 2 * half;
+  int rc = bdgd_gram_tasks(c, prec, cplx, 4, t, (int)k, d_out);
+  return rc;
+}
 // ---------------------------------------------------------------------------
 // residuals and column norms
 // ---------------------------------------------------------------------------
@@ -256,13 +330,14 @@ __device__ __forceinline__ void block_store(double v, double *part, int col, int
 template <typename T>
 __global__ void k_residual(const T *__restrict__ X, const T *__restrict__ AX, long long ld, T *__restrict__ Rout,
                            long long ldr, const double *__restrict__ lam, long long half_el, double *part_r,
-                           double *part_x) {
+                           double *part_x, const int *__restrict__ colmap) {
   const int col = blockIdx.y;
+  const int src = colmap ? colmap[col] : col;
   const int nb = gridDim.x;
-  const T *x = X + col * ld;
-  const T *ax = AX + col * ld;
+  const T *x = X + src * ld;
+  const T *ax = AX + src * ld;
   T *r = Rout ? Rout + col * ldr : nullptr;
-  const double l = lam[col];
+  const double l = lam[src];
   const long long n_el = 2 * half_el;
   double sr = 0.0, sx = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_el; i += (long long)nb * blockDim.x) {
@@ -314,7 +389,7 @@ static int norm_blocks(long long n) {
 
 extern "C" int bdgd_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half, uint64_t ncol, const void *d_X,
                              const void *d_AX, uint64_t ld, void *d_R, uint64_t ldr, const double *d_lam,
-                             double *d_work, double *d_rr, double *d_xx) {
+                             double *d_work, double *d_rr, double *d_xx, const int *d_colmap) {
   const int es = cplx ? 2 : 1;
   const long long half_el = (long long)half * es;
   const int nb = norm_blocks(2 * half_el);
@@ -322,10 +397,10 @@ extern "C" int bdgd_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half, uin
   dim3 grid(nb, (unsigned)ncol);
   if (prec == BDGD_F32)
     k_residual<float><<<grid, 256, 0, c->stream>>>((const float *)d_X, (const float *)d_AX, (long long)ld * es,
-                                                   (float *)d_R, (long long)ldr * es, d_lam, half_el, pr, px);
+                                                   (float *)d_R, (long long)ldr * es, d_lam, half_el, pr, px, d_colmap);
   else
     k_residual<double><<<grid, 256, 0, c->stream>>>((const double *)d_X, (const double *)d_AX, (long long)ld * es,
-                                                    (double *)d_R, (long long)ldr * es, d_lam, half_el, pr, px);
+                                                    (double *)d_R, (long long)ldr * es, d_lam, half_el, pr, px, d_colmap);
   BDGD_CK(cudaGetLastError());
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(pr, nb, (int)ncol, d_rr);
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(px, nb, (int)ncol, d_xx);
@@ -384,36 +459,38 @@ extern "C" int bdgd_convert(bdgd_ctx *c, int to_f32, const void *src, void *dst,
 // small dense helpers for the Rayleigh-Ritz step (k <= a few hundred)
 // matrices column-major, leading dimension = rows; complex interleaved.
 // ---------------------------------------------------------------------------
-// G = Guu + Gvv, Gb = Guv + Guv^H, Ga = (Ga + Ga^H)/2, Gs = D G D with
-// D = diag(G)^-1/2 (d returned).
-__global__ void k_rr_prepare(const double *__restrict__ gram, int k, int cplx, double *__restrict__ Gs,
+// From the Gram outputs G = S^H S, Ga = S^H A S, Guv = S_u^H S_v (k x k,
+// leading dimension ldo): Gs = D G D with D = diag(G)^-1/2 (d returned),
+// Gb = Guv + Guv^H, Ga <- (Ga + Ga^H)/2.  G may be null when only the
+// scaling of another matrix is wanted (then d is computed from Gs input).
+__global__ void k_rr_prepare(const double *__restrict__ G, const double *__restrict__ Gain,
+                             const double *__restrict__ Guv, int k, int ldo, int cplx, double *__restrict__ Gs,
                              double *__restrict__ Gb, double *__restrict__ Ga, double *__restrict__ d) {
   const long long kk = (long long)k * k;
   const int es = cplx ? 2 : 1;
-  const double *Guu = gram, *Gvv = gram + kk * es, *Guv = gram + 2 * kk * es, *Gaa = gram + 3 * kk * es;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < kk; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % k), j = (int)(q / k);
-    const long long ij = (long long)j * k + i, ji = (long long)i * k + j;
-    const double dii = Guu[((long long)i * k + i) * es] + Gvv[((long long)i * k + i) * es];
-    const double djj = Guu[((long long)j * k + j) * es] + Gvv[((long long)j * k + j) * es];
-    const double di = dii > 0 ? 1.0 / sqrt(dii) : 1.0;
-    const double dj = djj > 0 ? 1.0 / sqrt(djj) : 1.0;
+    const long long ij = (long long)j * ldo + i, ji = (long long)i * ldo + j;
+    const long long oij = (long long)j * k + i;
+    const double gii = G[((long long)i * ldo + i) * es], gjj = G[((long long)j * ldo + j) * es];
+    const double di = gii > 0 ? 1.0 / sqrt(gii) : 1.0;
+    const double dj = gjj > 0 ? 1.0 / sqrt(gjj) : 1.0;
     if (j == 0) d[i] = di;
     if (!cplx) {
-      const double g = 0.5 * ((Guu[ij] + Gvv[ij]) + (Guu[ji] + Gvv[ji]));
-      Gs[ij] = di * g * dj;
-      Gb[ij] = Guv[ij] + Guv[ji];
-      Ga[ij] = 0.5 * (Gaa[ij] + Gaa[ji]);
+      Gs[oij] = di * (0.5 * (G[ij] + G[ji])) * dj;
+      if (Gb) Gb[oij] = Guv[ij] + Guv[ji];
+      if (Ga) Ga[oij] = 0.5 * (Gain[ij] + Gain[ji]);
     } else {
-      // Hermitian parts: (M + M^H)/2, and Guv + Guv^H
-      const double gre = 0.5 * ((Guu[2 * ij] + Gvv[2 * ij]) + (Guu[2 * ji] + Gvv[2 * ji]));
-      const double gim = 0.5 * ((Guu[2 * ij + 1] + Gvv[2 * ij + 1]) - (Guu[2 * ji + 1] + Gvv[2 * ji + 1]));
-      Gs[2 * ij] = di * gre * dj;
-      Gs[2 * ij + 1] = di * gim * dj;
-      Gb[2 * ij] = Guv[2 * ij] + Guv[2 * ji];
-      Gb[2 * ij + 1] = Guv[2 * ij + 1] - Guv[2 * ji + 1];
-      Ga[2 * ij] = 0.5 * (Gaa[2 * ij] + Gaa[2 * ji]);
-      Ga[2 * ij + 1] = 0.5 * (Gaa[2 * ij + 1] - Gaa[2 * ji + 1]);
+      Gs[2 * oij] = di * (0.5 * (G[2 * ij] + G[2 * ji])) * dj;
+      Gs[2 * oij + 1] = di * (0.5 * (G[2 * ij + 1] - G[2 * ji + 1])) * dj;
+      if (Gb) {
+        Gb[2 * oij] = Guv[2 * ij] + Guv[2 * ji];
+        Gb[2 * oij + 1] = Guv[2 * ij + 1] - Guv[2 * ji + 1];
+      }
+      if (Ga) {
+        Ga[2 * oij] = 0.5 * (Gain[2 * ij] + Gain[2 * ji]);
+        Ga[2 * oij + 1] = 0.5 * (Gain[2 * ij + 1] - Gain[2 * ji + 1]);
+      }
     }
   }
 }
@@ -475,9 +552,9 @@ static int grid_for(long long n) {
   return (int)(b < 1 ? 1 : b);
 }
 
-extern "C" int bdgd_rr_prepare(bdgd_ctx *c, const double *gram, int k, int cplx, double *Gs, double *Gb, double *Ga,
-                               double *d) {
-  k_rr_prepare<<<grid_for((long long)k * k), 256, 0, c->stream>>>(gram, k, cplx, Gs, Gb, Ga, d);
+extern "C" int bdgd_rr_prepare(bdgd_ctx *c, const double *G, const double *Ga_in, const double *Guv, int k, int ldo,
+                               int cplx, double *Gs, double *Gb, double *Ga, double *d) {
+  k_rr_prepare<<<grid_for((long long)k * k), 256, 0, c->stream>>>(G, Ga_in, Guv, k, ldo, cplx, Gs, Gb, Ga, d);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
@@ -498,6 +575,37 @@ extern "C" int bdgd_hermitize(bdgd_ctx *c, double *A, int k, int cplx) {
 
 extern "C" int bdgd_clamp(bdgd_ctx *c, double *w, int n, double floor_rel) {
   k_clamp<<<1, 256, 0, c->stream>>>(w, n, floor_rel);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+// out[i] = in[i]^e for in[i] > 0, else 0
+__global__ void k_vec_pow(const double *__restrict__ in, int n, double e, double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = in[i] > 0 ? pow(in[i], e) : 0.0;
+}
+
+extern "C" int bdgd_vec_pow(bdgd_ctx *c, const double *in, int n, double e, double *out) {
+  k_vec_pow<<<(n + 255) / 256, 256, 0, c->stream>>>(in, n, e, out);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+// Out[:, j] = In[:, cols[j]] (rows x ncols, FP64 or complex, leading dims ldi / ldo)
+__global__ void k_gather_cols(const double *__restrict__ In, int ldi, int rows, const int *__restrict__ cols,
+                              int ncols, int cplx, double *__restrict__ Out, int ldo) {
+  const int es = cplx ? 2 : 1;
+  const long long tot = (long long)rows * ncols;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % rows), j = (int)(q / rows);
+    for (int e = 0; e < es; ++e) Out[((long long)j * ldo + i) * es + e] = In[((long long)cols[j] * ldi + i) * es + e];
+  }
+}
+
+extern "C" int bdgd_gather_cols(bdgd_ctx *c, const double *In, int ldi, int rows, const int *d_cols, int ncols,
+                                int cplx, double *Out, int ldo) {
+  k_gather_cols<<<grid_for((long long)rows * ncols), 256, 0, c->stream>>>(In, ldi, rows, d_cols, ncols, cplx, Out,
+                                                                           ldo);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }

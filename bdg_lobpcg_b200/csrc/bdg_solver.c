@@ -6,24 +6,31 @@
  * an unvendored "LOBPCG" library).  The iteration is restated from the
  * published method (Kressner, Miloloza Pandur & Shao, "An indefinite variant
  * of LOBPCG for definite matrix pencils", Numer. Algorithms 66, 2014) in
- * block form for the pencil (A, B) = (diag(K, M), swap):
+ * block form for the pencil (A, B) = (diag(K, M), swap), with the basis
+ * hygiene of robust LOBPCG implementations:
  *
  *   X0 (B-positive) -> AX = A X -> Rayleigh-Ritz on span X
- *   repeat:  R = AX - B X diag(lam)          (swap folded into the kernel)
- *            test the nev wanted pairs       (backward error or ||KMv - w^2 v||)
- *            W = T R,  AW = A W              (batched FFT operator kernels)
- *            Gram blocks of S = [X W P]      (FP64 tensor-core contraction)
- *            Rayleigh-Ritz on the projected definite pencil:
- *              S^H S = Guu + Gvv -> implicit orthonormalisation (small
- *              directions dropped), A_s = Q D Q^H (D clamped so a Goldstone
- *              null direction stays finite), H = D^-1/2 Q^H B_s Q D^-1/2,
+ *   repeat:  norms of R = AX - B X diag(lam) (swap folded into the kernel)
+ *            test the nev wanted pairs; active set = unconverged columns
+ *            W = T R_active                     (batched FFT operator kernels)
+ *            P <- P - X (X^H X)^+ X^H P, SVQB   (AP transformed alike)
+ *            W <- W - Q (Q^H Q)^+ Q^H W, SVQB   (Q = [X, P]),  AW = A W
+ *            Rayleigh-Ritz on S = [X, P, W] from the Gram blocks
+ *              S^H S, S^H A S, S_u^H S_v (FP64 tensor-core contraction;
+ *              S^H B S = S_u^H S_v + S_v^H S_u, B never touches memory):
+ *              implicit orthonormalisation (small directions dropped),
+ *              A_s = Q D Q^H (D clamped), H = D^-1/2 Q^H B_s Q D^-1/2,
  *              theta = eig(H), lam = 1/theta, the m largest positive theta
- *            X <- S C,  P <- [W P] C_wp  (and AX, AP alike, no extra apply)
+ *            X <- S C,  P <- [P, W] C_pw (active columns); AX, AP alike
  *
- * Everything block-sized stays in HBM for the whole solve; the host sees
- * only the k x k eigenvalue counts and the convergence norms each iteration.
- * Block updates are plain GEMMs (cuBLAS); the k x k eigenproblems use
- * cuSOLVER syevd/heevd.
+ * Every block lives in HBM for the whole solve; per iteration the host
+ * reads the Ritz values, a few small eigenvalue spectra (for the drop
+ * decisions) and the residual norms.  Block updates are plain GEMMs
+ * (cuBLAS); the small Hermitian eigenproblems use cuSOLVER.
+ *
+ * BDG_PREC_MIXED runs the same iteration with FP32 blocks and FP32 operator
+ * applies (Gram accumulation and all small dense work stay FP64) until the
+ * FP32 floor, then continues in FP64 from the converted block.
  */
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
@@ -36,47 +43,61 @@
 #include "bdg/bdg_internal.h"
 #include "bdg_blas.h"
 
-#define RR_DROP_F64 1e-13
-#define RR_DROP_F32 1e-6
-#define RR_CLAMP 1e-14
+#define DROP_F64 1e-13
+#define DROP_F32 1e-7
+#define CLAMP_A 1e-14
+#define GUARD_LOCK 1e-12
+#define MIXED_SWITCH 2e-6 /* backward error at which FP32 blocks hand over to FP64 */
+
+enum { NB_X, NB_AX, NB_XN, NB_AXN, NB_P, NB_AP, NB_PN, NB_APN, NB_W, NB_AW, NB_R, NB_WT, NB_T1, NB_T2, NB_COUNT };
 
 typedef struct {
-  uint64_t S, n, m, nev, kmax;
+  uint64_t S, n, m, nev;
   int cplx;
-  int prec;      /* BDGD_F64 / BDGD_F32 storage of the current blocks */
-  size_t esz;    /* bytes per block element */
-  void *S0, *S1, *AS0, *AS1, *R, *TR, *X64; /* TR: S x nev; X64: FP64 copy for refinement */
-  double *lam, *work, *norms, *gram, *Gs, *Gb, *Ga, *dsc, *Z, *T1, *T2, *Ga2, *Gb2, *Y, *H, *V, *C64, *wG, *wA, *wH;
+  int prec;
+  size_t esz;
+  void *blk[NB_COUNT];
+  void *TR;      /* S x nev, true-residual scratch */
+  int p;         /* columns in P (0: none yet) */
+  /* small dense (FP64, device) */
+  int K;         /* 3m */
+  double *gout;  /* 3 Gram outputs, K x K */
+  double *Gs, *Gb, *Ga, *Z, *Ya, *Hh, *V, *C, *Cs, *T1s, *T2s, *dsc, *wG, *wA, *wH, *wtmp, *lam_d, *work, *norms;
   float *C32;
-  double *defl; /* deflation vectors psi0 and w (FP64, [2][n_half*es]) */
+  int *colmap, *actcols;
+  double *defl;  /* psi0 and w = M^-1 psi0 (block precision), n_half each */
+  double wpsi;   /* w^H psi0 */
+  int deflate;
   cublasHandle_t blas;
   cusolverDnHandle_t sol;
   void *swork;
   int lwork;
   int *info;
-  size_t bytes_blocks;
   uint64_t cap_S, cap_m, cap_nev;
   int cap_cplx, cap_prec;
-  cudaEvent_t ev[16];
+  cudaEvent_t ev[12];
 } ws_t;
 
 static void ws_free(ws_t *w) {
   if (!w) return;
-  void *bufs[] = {w->S0, w->S1, w->AS0, w->AS1, w->R, w->TR, w->X64, w->lam, w->work, w->norms, w->gram, w->Gs,
-                  w->Gb, w->Ga, w->dsc, w->Z,   w->T1, w->T2, w->Ga2, w->Gb2, w->Y, w->H, w->V, w->C64, w->wG,
-                  w->wA, w->wH, w->C32, w->defl, w->swork, w->info};
+  for (int i = 0; i < NB_COUNT; i++)
+    if (w->blk[i]) cudaFree(w->blk[i]);
+  void *bufs[] = {w->TR, w->gout, w->Gs, w->Gb, w->Ga, w->Z, w->Ya, w->Hh, w->V, w->C, w->Cs, w->T1s, w->T2s,
+                  w->dsc, w->wG, w->wA, w->wH, w->wtmp, w->lam_d, w->work, w->norms, w->C32, w->colmap,
+                  w->actcols, w->defl, w->swork, w->info};
   for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; i++)
     if (bufs[i]) cudaFree(bufs[i]);
   if (w->blas) cublasDestroy(w->blas);
   if (w->sol) cusolverDnDestroy(w->sol);
-  for (int i = 0; i < 16; i++)
+  for (int i = 0; i < 12; i++)
     if (w->ev[i]) cudaEventDestroy(w->ev[i]);
   memset(w, 0, sizeof *w);
 }
 
 void bdg_solver_release(bdg_t *bdg) {
   if (bdg->solver_ws) {
-    ws_free((ws_t *)bdg->solver_ws);
+    ws_free(&((ws_t *)bdg->solver_ws)[0]);
+    ws_free(&((ws_t *)bdg->solver_ws)[1]);
     free(bdg->solver_ws);
     bdg->solver_ws = NULL;
   }
@@ -85,37 +106,42 @@ void bdg_solver_release(bdg_t *bdg) {
 
 const void *bdg_solver_block(const bdg_t *bdg) { return bdg->block; }
 
-#define CUDA_TRY(x)                                                                     \
-  do {                                                                                  \
-    cudaError_t _e = (x);                                                               \
-    if (_e != cudaSuccess) {                                                            \
-      fprintf(stderr, "bdg_solve: %s failed: %s\n", #x, cudaGetErrorString(_e));        \
-      return -1;                                                                        \
-    }                                                                                   \
+#define CUDA_TRY(x)                                                              \
+  do {                                                                           \
+    cudaError_t _e = (x);                                                        \
+    if (_e != cudaSuccess) {                                                     \
+      fprintf(stderr, "bdg_solve: %s failed: %s\n", #x, cudaGetErrorString(_e)); \
+      return -1;                                                                 \
+    }                                                                            \
   } while (0)
-#define BLAS_TRY(x)                                                                     \
-  do {                                                                                  \
-    cublasStatus_t _s = (x);                                                            \
-    if (_s != CUBLAS_STATUS_SUCCESS) {                                                  \
-      fprintf(stderr, "bdg_solve: %s failed: %d\n", #x, (int)_s);                       \
-      return -2;                                                                        \
-    }                                                                                   \
+#define BLAS_TRY(x)                                                \
+  do {                                                             \
+    cublasStatus_t _s = (x);                                       \
+    if (_s != CUBLAS_STATUS_SUCCESS) {                             \
+      fprintf(stderr, "bdg_solve: %s failed: %d\n", #x, (int)_s);  \
+      return -2;                                                   \
+    }                                                              \
   } while (0)
-#define SOL_TRY(x)                                                                      \
-  do {                                                                                  \
-    cusolverStatus_t _s = (x);                                                          \
-    if (_s != CUSOLVER_STATUS_SUCCESS) {                                                \
-      fprintf(stderr, "bdg_solve: %s failed: %d\n", #x, (int)_s);                       \
-      return -3;                                                                        \
-    }                                                                                   \
+#define SOL_TRY(x)                                                 \
+  do {                                                             \
+    cusolverStatus_t _s = (x);                                     \
+    if (_s != CUSOLVER_STATUS_SUCCESS) {                           \
+      fprintf(stderr, "bdg_solve: %s failed: %d\n", #x, (int)_s);  \
+      return -3;                                                   \
+    }                                                              \
   } while (0)
-#define DEV_TRY(x)                                                                      \
-  do {                                                                                  \
-    int _r = (x);                                                                       \
-    if (_r) {                                                                           \
-      fprintf(stderr, "bdg_solve: %s failed (%d): %s\n", #x, _r, bdgd_last_error());    \
-      return _r;                                                                        \
-    }                                                                                   \
+#define DEV_TRY(x)                                                                   \
+  do {                                                                               \
+    int _r = (x);                                                                    \
+    if (_r) {                                                                        \
+      fprintf(stderr, "bdg_solve: %s failed (%d): %s\n", #x, _r, bdgd_last_error()); \
+      return _r;                                                                     \
+    }                                                                                \
+  } while (0)
+#define TRY(x)              \
+  do {                      \
+    int _r = (x);           \
+    if (_r) return _r;      \
   } while (0)
 
 static int dmalloc(void **p, size_t bytes) {
@@ -123,176 +149,342 @@ static int dmalloc(void **p, size_t bytes) {
   return 0;
 }
 
+static cudaStream_t stream_of(bdgd_ctx *dev) { return (cudaStream_t)bdgd_stream(dev); }
+
 static int ws_setup(ws_t *w, bdgd_ctx *dev, uint64_t S, uint64_t m, uint64_t nev, int cplx, int prec) {
-  if (w->S0 && w->cap_S == S && w->cap_m == m && w->cap_nev == nev && w->cap_cplx == cplx && w->cap_prec == prec)
+  if (w->blk[0] && w->cap_S == S && w->cap_m == m && w->cap_nev == nev && w->cap_cplx == cplx &&
+      w->cap_prec == prec) {
+    w->p = 0;
     return 0;
+  }
   ws_free(w);
   w->S = S;
   w->n = 2 * S;
   w->m = m;
   w->nev = nev;
-  w->kmax = 3 * m;
   w->cplx = cplx;
   w->prec = prec;
-  w->esz = (prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
-  const size_t blk = w->n * w->kmax * w->esz;
-  int rc;
-  if ((rc = dmalloc(&w->S0, blk)) || (rc = dmalloc(&w->S1, blk)) || (rc = dmalloc(&w->AS0, blk)) ||
-      (rc = dmalloc(&w->AS1, blk)) || (rc = dmalloc(&w->R, w->n * m * w->esz)) ||
-      (rc = dmalloc(&w->TR, S * nev * w->esz)))
-    return rc;
+  w->esz = (size_t)(prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
+  w->K = (int)(3 * m);
+  for (int i = 0; i < NB_COUNT; i++) TRY(dmalloc(&w->blk[i], w->n * m * w->esz));
+  TRY(dmalloc(&w->TR, S * nev * w->esz));
   const size_t es = cplx ? 2 : 1;
-  const size_t kk = w->kmax * w->kmax * es * sizeof(double);
-  void **small[] = {(void **)&w->Gs, (void **)&w->Gb, (void **)&w->Ga, (void **)&w->Z, (void **)&w->T1,
-                    (void **)&w->T2, (void **)&w->Ga2, (void **)&w->Gb2, (void **)&w->Y, (void **)&w->H,
-                    (void **)&w->V, (void **)&w->C64};
-  for (size_t i = 0; i < sizeof small / sizeof small[0]; i++)
-    if ((rc = dmalloc(small[i], kk))) return rc;
-  if ((rc = dmalloc((void **)&w->C32, kk)) || (rc = dmalloc((void **)&w->gram, 4 * kk)) ||
-      (rc = dmalloc((void **)&w->lam, w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->work, 2 * 64 * w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->norms, 4 * w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->dsc, w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->wG, w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->wA, w->kmax * sizeof(double))) ||
-      (rc = dmalloc((void **)&w->wH, w->kmax * sizeof(double))) || (rc = dmalloc((void **)&w->info, sizeof(int))))
-    return rc;
+  const size_t kk = (size_t)w->K * w->K * es * sizeof(double);
+  TRY(dmalloc((void **)&w->gout, 3 * kk));
+  double **sm[] = {&w->Gs, &w->Gb, &w->Ga, &w->Z, &w->Ya, &w->Hh, &w->V, &w->C, &w->Cs, &w->T1s, &w->T2s};
+  for (size_t i = 0; i < sizeof sm / sizeof sm[0]; i++) TRY(dmalloc((void **)sm[i], kk));
+  TRY(dmalloc((void **)&w->C32, kk));
+  double **vec[] = {&w->dsc, &w->wG, &w->wA, &w->wH, &w->wtmp, &w->lam_d};
+  for (size_t i = 0; i < sizeof vec / sizeof vec[0]; i++) TRY(dmalloc((void **)vec[i], (size_t)w->K * sizeof(double)));
+  TRY(dmalloc((void **)&w->work, 2 * 64 * (size_t)w->K * sizeof(double)));
+  TRY(dmalloc((void **)&w->norms, 4 * (size_t)w->K * sizeof(double)));
+  TRY(dmalloc((void **)&w->colmap, (size_t)w->K * sizeof(int)));
+  TRY(dmalloc((void **)&w->actcols, (size_t)w->K * sizeof(int)));
+  TRY(dmalloc((void **)&w->info, sizeof(int)));
   BLAS_TRY(cublasCreate(&w->blas));
-  BLAS_TRY(cublasSetStream(w->blas, (cudaStream_t)bdgd_stream(dev)));
+  BLAS_TRY(cublasSetStream(w->blas, stream_of(dev)));
   SOL_TRY(cusolverDnCreate(&w->sol));
-  SOL_TRY(cusolverDnSetStream(w->sol, (cudaStream_t)bdgd_stream(dev)));
+  SOL_TRY(cusolverDnSetStream(w->sol, stream_of(dev)));
   int lw = 0;
-  const int K = (int)w->kmax;
   if (cplx) {
-    SOL_TRY(cusolverDnZheevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K,
-                                        (cuDoubleComplex *)w->Gs, K, w->wG, &lw));
+    SOL_TRY(cusolverDnZheevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, w->K,
+                                        (cuDoubleComplex *)w->Gs, w->K, w->wG, &lw));
     w->lwork = lw;
-    if ((rc = dmalloc(&w->swork, (size_t)lw * sizeof(cuDoubleComplex)))) return rc;
+    TRY(dmalloc(&w->swork, (size_t)lw * sizeof(cuDoubleComplex)));
   } else {
-    SOL_TRY(cusolverDnDsyevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, w->Gs, K,
+    SOL_TRY(cusolverDnDsyevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, w->K, w->Gs, w->K,
                                         w->wG, &lw));
     w->lwork = lw;
-    if ((rc = dmalloc(&w->swork, (size_t)lw * sizeof(double)))) return rc;
+    TRY(dmalloc(&w->swork, (size_t)lw * sizeof(double)));
   }
-  for (int i = 0; i < 16; i++) CUDA_TRY(cudaEventCreate(&w->ev[i]));
+  for (int i = 0; i < 12; i++) CUDA_TRY(cudaEventCreate(&w->ev[i]));
   w->cap_S = S;
   w->cap_m = m;
   w->cap_nev = nev;
   w->cap_cplx = cplx;
   w->cap_prec = prec;
+  w->p = 0;
   return 0;
 }
 
-/* Hermitian eigen-decomposition in place (eigenvalues ascending). */
-static int heev(ws_t *w, double *A, int k, double *wout) {
+#define B(i) (w->blk[i])
+static inline void *colp(ws_t *w, void *base, uint64_t col) { return (char *)base + col * w->n * w->esz; }
+static inline void swapb(ws_t *w, int a, int b) {
+  void *t = w->blk[a];
+  w->blk[a] = w->blk[b];
+  w->blk[b] = t;
+}
+
+/* ---- small dense FP64 helpers (device) ------------------------------------ */
+static int heev(ws_t *w, double *A, int k, int lda, double *ev) {
+  if (k <= 0) return 0;
   if (w->cplx)
-    SOL_TRY(cusolverDnZheevd(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, (cuDoubleComplex *)A, k,
-                             wout, (cuDoubleComplex *)w->swork, w->lwork, w->info));
+    SOL_TRY(cusolverDnZheevd(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, (cuDoubleComplex *)A, lda,
+                             ev, (cuDoubleComplex *)w->swork, w->lwork, w->info));
   else
-    SOL_TRY(cusolverDnDsyevd(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, A, k, wout,
+    SOL_TRY(cusolverDnDsyevd(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, A, lda, ev,
                              (double *)w->swork, w->lwork, w->info));
   return 0;
 }
 
-/* small FP64 GEMM: C = op(A) op(B), op = N or H */
-static int sgemm_small(ws_t *w, int ha, int hb, int M, int N, int K, const double *A, int lda, const double *B,
-                       int ldb, double *C, int ldc) {
+/* C = alpha op(A) op(B) + beta C, op = N or H */
+static int zgemm_small(ws_t *w, int ha, int hb, int M, int N, int K, double alpha, const double *A, int lda,
+                       const double *Bm, int ldb, double beta, double *Cm, int ldc) {
+  if (M <= 0 || N <= 0) return 0;
   if (w->cplx) {
-    const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0};
-    BLAS_TRY(cublasZgemm(w->blas, ha ? CUBLAS_OP_C : CUBLAS_OP_N, hb ? CUBLAS_OP_C : CUBLAS_OP_N, M, N, K, &one,
-                         (const cuDoubleComplex *)A, lda, (const cuDoubleComplex *)B, ldb, &zero,
-                         (cuDoubleComplex *)C, ldc));
+    const cuDoubleComplex a = {alpha, 0.0}, b = {beta, 0.0};
+    BLAS_TRY(cublasZgemm(w->blas, ha ? CUBLAS_OP_C : CUBLAS_OP_N, hb ? CUBLAS_OP_C : CUBLAS_OP_N, M, N, K, &a,
+                         (const cuDoubleComplex *)A, lda, (const cuDoubleComplex *)Bm, ldb, &b,
+                         (cuDoubleComplex *)Cm, ldc));
   } else {
-    const double one = 1.0, zero = 0.0;
-    BLAS_TRY(cublasDgemm(w->blas, ha ? CUBLAS_OP_T : CUBLAS_OP_N, hb ? CUBLAS_OP_T : CUBLAS_OP_N, M, N, K, &one, A,
-                         lda, B, ldb, &zero, C, ldc));
+    BLAS_TRY(cublasDgemm(w->blas, ha ? CUBLAS_OP_T : CUBLAS_OP_N, hb ? CUBLAS_OP_T : CUBLAS_OP_N, M, N, K, &alpha,
+                         A, lda, Bm, ldb, &beta, Cm, ldc));
   }
   return 0;
 }
 
-/* Rayleigh-Ritz on the Gram blocks in w->gram (k x k).  On return w->C64
- * holds C (k x m), lam_host the m eigenvalues (ascending), *nsel the number
- * selected. */
-static int rayleigh_ritz(ws_t *w, bdgd_ctx *dev, int k, int m, double drop, double *lam_host, int *nsel) {
-  cudaStream_t st = (cudaStream_t)bdgd_stream(dev);
-  const int cplx = w->cplx;
-  const size_t es = cplx ? 2 : 1;
-  DEV_TRY(bdgd_rr_prepare(dev, w->gram, k, cplx, w->Gs, w->Gb, w->Ga, w->dsc));
-  int rc;
-  if ((rc = heev(w, w->Gs, k, w->wG))) return rc;
-  double hw[3 * 1024];
-  if (k > 3 * 1024) return -4;
-  CUDA_TRY(cudaMemcpyAsync(hw, w->wG, k * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  const double smax = hw[k - 1];
-  int keep = 0;
-  for (int i = 0; i < k; i++)
-    if (hw[i] > drop * smax) keep++;
-  if (keep < m) keep = (m <= k) ? m : k;
-  /* Z = D Q[:, k-keep:] diag(s^-1/2) */
-  DEV_TRY(bdgd_scale_cols(dev, w->Gs, k, k - keep, keep, cplx, w->dsc, w->wG, 1, 0, w->Z));
-  if ((rc = sgemm_small(w, 0, 0, k, keep, k, w->Ga, k, w->Z, k, w->T1, k))) return rc;
-  if ((rc = sgemm_small(w, 1, 0, keep, keep, k, w->Z, k, w->T1, k, w->Ga2, keep))) return rc;
-  if ((rc = sgemm_small(w, 0, 0, k, keep, k, w->Gb, k, w->Z, k, w->T1, k))) return rc;
-  if ((rc = sgemm_small(w, 1, 0, keep, keep, k, w->Z, k, w->T1, k, w->Gb2, keep))) return rc;
-  DEV_TRY(bdgd_hermitize(dev, w->Ga2, keep, cplx));
-  DEV_TRY(bdgd_hermitize(dev, w->Gb2, keep, cplx));
-  if ((rc = heev(w, w->Ga2, keep, w->wA))) return rc;
-  DEV_TRY(bdgd_clamp(dev, w->wA, keep, RR_CLAMP));
-  /* Y = Q2 diag(dA^-1/2); H = Y^H Gb2 Y */
-  DEV_TRY(bdgd_scale_cols(dev, w->Ga2, keep, 0, keep, cplx, NULL, w->wA, 1, 0, w->Y));
-  if ((rc = sgemm_small(w, 0, 0, keep, keep, keep, w->Gb2, keep, w->Y, keep, w->T1, keep))) return rc;
-  if ((rc = sgemm_small(w, 1, 0, keep, keep, keep, w->Y, keep, w->T1, keep, w->H, keep))) return rc;
-  DEV_TRY(bdgd_hermitize(dev, w->H, keep, cplx));
-  if ((rc = heev(w, w->H, keep, w->wH))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(hw, w->wH, keep * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  int npos = 0;
-  for (int i = 0; i < keep; i++)
-    if (hw[i] > 0) npos++;
-  const int sel = npos < m ? npos : m;
-  *nsel = sel;
-  if (sel == 0) return 0;
-  /* V = Q3[:, largest theta first] diag(theta^-1/2); C = Z Y V */
-  DEV_TRY(bdgd_scale_cols(dev, w->H, keep, keep - sel, sel, cplx, NULL, w->wH, 1, 1, w->V));
-  if ((rc = sgemm_small(w, 0, 0, keep, sel, keep, w->Y, keep, w->V, keep, w->T2, keep))) return rc;
-  if ((rc = sgemm_small(w, 0, 0, k, sel, keep, w->Z, k, w->T2, keep, w->C64, k))) return rc;
-  for (int j = 0; j < sel; j++) lam_host[j] = 1.0 / hw[keep - 1 - j];
-  (void)es;
+static int host_vec(ws_t *w, bdgd_ctx *dev, const double *d, int n, double *h) {
+  CUDA_TRY(cudaMemcpyAsync(h, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_of(dev)));
+  CUDA_TRY(cudaStreamSynchronize(stream_of(dev)));
   return 0;
 }
 
-/* Y[:, 0:ncol] = X[:, 0:k] C (C is k x ncol FP64 on device, leading dim ldc).
- * X, Y blocks of the current precision with leading dimension n. */
-static int block_gemm(ws_t *w, bdgd_ctx *dev, const void *X, int k, const double *C, int ldc, int ncol, void *Y) {
+/* Scaled eigen-decomposition of a Hermitian Gram block G (k x k, leading dim
+ * ldg): Gs = D G D in w->Gs (eigenvectors after the call), eigenvalues in
+ * w->wG (ascending), D in w->dsc; returns the count kept (> drop * max) in
+ * *keep; the kept vectors are the last *keep columns. */
+static int scaled_eig(ws_t *w, bdgd_ctx *dev, const double *G, int k, int ldg, double drop, int *keep) {
+  DEV_TRY(bdgd_rr_prepare(dev, G, NULL, NULL, k, ldg, w->cplx, w->Gs, NULL, NULL, w->dsc));
+  TRY(heev(w, w->Gs, k, k, w->wG));
+  double h[3 * 1024];
+  TRY(host_vec(w, dev, w->wG, k, h));
+  const double smax = h[k - 1];
+  int c = 0;
+  for (int i = 0; i < k; i++)
+    if (h[i] > drop * smax) c++;
+  *keep = c;
+  return 0;
+}
+
+/* Z (k x keep) with Z^H G Z = I: SVQB coefficients. */
+static int svqb(ws_t *w, bdgd_ctx *dev, const double *G, int k, int ldg, double drop, double *Zout, int *keep) {
+  TRY(scaled_eig(w, dev, G, k, ldg, drop, keep));
+  DEV_TRY(bdgd_scale_cols(dev, w->Gs, k, k - *keep, *keep, w->cplx, w->dsc, w->wG, 1, 0, Zout));
+  return 0;
+}
+
+/* Y = G^+ Bm  (G: k x k Gram, Bm: k x q, both leading dim ld), into Yout (k x q, ld k). */
+static int gram_pinv_apply(ws_t *w, bdgd_ctx *dev, const double *G, int k, int ld, const double *Bm, int q,
+                           double drop, double *Yout) {
+  int keep = 0;
+  TRY(scaled_eig(w, dev, G, k, ld, drop, &keep));
+  if (keep == 0 || q == 0) {
+    CUDA_TRY(cudaMemsetAsync(Yout, 0, (size_t)k * q * (w->cplx ? 2 : 1) * sizeof(double), stream_of(dev)));
+    return 0;
+  }
+  /* U = D Q_keep s^-1/2 ; Y = U U^H Bm */
+  DEV_TRY(bdgd_scale_cols(dev, w->Gs, k, k - keep, keep, w->cplx, w->dsc, w->wG, 1, 0, w->Z));
+  TRY(zgemm_small(w, 1, 0, keep, q, k, 1.0, w->Z, k, Bm, ld, 0.0, w->T1s, keep));
+  TRY(zgemm_small(w, 0, 0, k, q, keep, 1.0, w->Z, k, w->T1s, keep, 0.0, Yout, k));
+  return 0;
+}
+
+/* ---- block GEMMs (block precision) ---------------------------------------- */
+/* Y = alpha * X[:, 0:k] Cm + beta * Y; Cm FP64 k x ncol with leading dim ldc. */
+static int bgemm(ws_t *w, bdgd_ctx *dev, const void *X, int k, const double *Cm, int ldc, int ncol, double alpha,
+                 double beta, void *Y) {
+  if (k <= 0 || ncol <= 0) return 0;
   const int n = (int)w->n;
   if (w->prec == BDGD_F32) {
-    /* C -> float (k x ncol, leading dim k) */
-    DEV_TRY(bdgd_scale_cols(dev, C, ldc, 0, ncol, w->cplx, NULL, NULL, 0, 0, w->T1));
-    DEV_TRY(bdgd_convert(dev, 1, w->T1, w->C32, (uint64_t)ldc * ncol * (w->cplx ? 2 : 1)));
+    DEV_TRY(bdgd_scale_cols(dev, Cm, ldc, 0, ncol, w->cplx, NULL, NULL, 0, 0, w->T2s));
+    DEV_TRY(bdgd_convert(dev, 1, w->T2s, w->C32, (uint64_t)ldc * ncol * (w->cplx ? 2 : 1)));
     if (w->cplx) {
-      const cuComplex one = {1.f, 0.f}, zero = {0.f, 0.f};
-      BLAS_TRY(cublasCgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &one, (const cuComplex *)X, n,
-                           (const cuComplex *)w->C32, ldc, &zero, (cuComplex *)Y, n));
+      const cuComplex a = {(float)alpha, 0.f}, b = {(float)beta, 0.f};
+      BLAS_TRY(cublasCgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &a, (const cuComplex *)X, n,
+                           (const cuComplex *)w->C32, ldc, &b, (cuComplex *)Y, n));
     } else {
-      const float one = 1.f, zero = 0.f;
-      BLAS_TRY(cublasSgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &one, (const float *)X, n, w->C32, ldc,
-                           &zero, (float *)Y, n));
+      const float a = (float)alpha, b = (float)beta;
+      BLAS_TRY(cublasSgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &a, (const float *)X, n, w->C32, ldc, &b,
+                           (float *)Y, n));
     }
   } else if (w->cplx) {
-    const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0};
-    BLAS_TRY(cublasZgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &one, (const cuDoubleComplex *)X, n,
-                         (const cuDoubleComplex *)C, ldc, &zero, (cuDoubleComplex *)Y, n));
+    const cuDoubleComplex a = {alpha, 0.0}, b = {beta, 0.0};
+    BLAS_TRY(cublasZgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &a, (const cuDoubleComplex *)X, n,
+                         (const cuDoubleComplex *)Cm, ldc, &b, (cuDoubleComplex *)Y, n));
   } else {
-    const double one = 1.0, zero = 0.0;
-    BLAS_TRY(cublasDgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &one, (const double *)X, n, C, ldc, &zero,
+    BLAS_TRY(cublasDgemm(w->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, k, &alpha, (const double *)X, n, Cm, ldc, &beta,
                          (double *)Y, n));
   }
   return 0;
 }
 
-static inline void *col_ptr(ws_t *w, void *base, uint64_t col) { return (char *)base + col * w->n * w->esz; }
+/* ---- Gram launches ---------------------------------------------------------- */
+static bdgd_gram_task mk_task(ws_t *w, const void *a, const void *b, uint64_t rows, int ka, int kb, int out, int i0,
+                              int j0, int sym, int mirror) {
+  bdgd_gram_task t;
+  t.a = a;
+  t.b = b;
+  t.lda = w->n;
+  t.ldb = w->n;
+  t.rows = rows;
+  t.ka = ka;
+  t.kb = kb;
+  t.out = out;
+  t.i0 = i0;
+  t.j0 = j0;
+  t.sym = sym;
+  t.mirror = mirror;
+  return t;
+}
 
+/* Rayleigh-Ritz Grams of S = [blocks] (with A-images): out0 = S^H S, out1 =
+ * S^H A S, out2 = S_u^H S_v, all K x K leading dim K at w->gout. */
+static int rr_grams(ws_t *w, bdgd_ctx *dev, int nb, void *const *Sb, void *const *ASb, const int *kb) {
+  bdgd_gram_task t[48];
+  int nt = 0, off[4];
+  off[0] = 0;
+  for (int i = 0; i < nb; i++) off[i + 1] = off[i] + kb[i];
+  const size_t hb = w->S * w->esz;
+  for (int i = 0; i < nb; i++)
+    for (int j = i; j < nb; j++) {
+      if (!kb[i] || !kb[j]) continue;
+      t[nt++] = mk_task(w, Sb[i], Sb[j], w->n, kb[i], kb[j], 0, off[i], off[j], i == j, i != j);
+      t[nt++] = mk_task(w, Sb[i], ASb[j], w->n, kb[i], kb[j], 1, off[i], off[j], i == j, i != j);
+    }
+  for (int i = 0; i < nb; i++)
+    for (int j = 0; j < nb; j++) {
+      if (!kb[i] || !kb[j]) continue;
+      t[nt++] = mk_task(w, Sb[i], (const char *)Sb[j] + hb, w->S, kb[i], kb[j], 2, off[i], off[j], 0, 0);
+    }
+  DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, nt, t, w->K, w->gout));
+  return 0;
+}
+
+/* Rayleigh-Ritz of the pencil on the Gram outputs (k x k): on return w->C
+ * holds C (k x m, leading dim k), lam[] the m Ritz values (ascending), *nsel
+ * the number of positive-type values selected. */
+static int rayleigh_ritz(ws_t *w, bdgd_ctx *dev, int k, int m, double drop, double *lam, int *nsel) {
+  const int K = w->K, cplx = w->cplx;
+  const size_t es = cplx ? 2 : 1;
+  const double *G = w->gout, *Gain = w->gout + (size_t)K * K * es, *Guv = w->gout + 2 * (size_t)K * K * es;
+  DEV_TRY(bdgd_rr_prepare(dev, G, Gain, Guv, k, K, cplx, w->Gs, w->Gb, w->Ga, w->dsc));
+  TRY(heev(w, w->Gs, k, k, w->wG));
+  double h[3 * 1024];
+  TRY(host_vec(w, dev, w->wG, k, h));
+  const double smax = h[k - 1];
+  int keep = 0;
+  for (int i = 0; i < k; i++)
+    if (h[i] > drop * smax) keep++;
+  if (keep < m) keep = m <= k ? m : k;
+  /* Z = D Q[:, k-keep:] diag(s^-1/2) (orthonormalises S implicitly) */
+  DEV_TRY(bdgd_scale_cols(dev, w->Gs, k, k - keep, keep, cplx, w->dsc, w->wG, 1, 0, w->Z));
+  /* A_s and B_s on the orthonormal basis */
+  TRY(zgemm_small(w, 0, 0, k, keep, k, 1.0, w->Ga, k, w->Z, k, 0.0, w->T1s, k));
+  TRY(zgemm_small(w, 1, 0, keep, keep, k, 1.0, w->Z, k, w->T1s, k, 0.0, w->Ya, keep));
+  TRY(zgemm_small(w, 0, 0, k, keep, k, 1.0, w->Gb, k, w->Z, k, 0.0, w->T1s, k));
+  TRY(zgemm_small(w, 1, 0, keep, keep, k, 1.0, w->Z, k, w->T1s, k, 0.0, w->Hh, keep));
+  DEV_TRY(bdgd_hermitize(dev, w->Ya, keep, cplx));
+  DEV_TRY(bdgd_hermitize(dev, w->Hh, keep, cplx));
+  TRY(heev(w, w->Ya, keep, keep, w->wA));
+  DEV_TRY(bdgd_clamp(dev, w->wA, keep, CLAMP_A));
+  /* Y = Q2 diag(dA^-1/2);  H = Y^H B_s Y */
+  DEV_TRY(bdgd_scale_cols(dev, w->Ya, keep, 0, keep, cplx, NULL, w->wA, 1, 0, w->V));
+  TRY(zgemm_small(w, 0, 0, keep, keep, keep, 1.0, w->Hh, keep, w->V, keep, 0.0, w->T1s, keep));
+  TRY(zgemm_small(w, 1, 0, keep, keep, keep, 1.0, w->V, keep, w->T1s, keep, 0.0, w->Ya, keep));
+  DEV_TRY(bdgd_hermitize(dev, w->Ya, keep, cplx));
+  TRY(heev(w, w->Ya, keep, keep, w->wH));
+  TRY(host_vec(w, dev, w->wH, keep, h));
+  int npos = 0;
+  for (int i = 0; i < keep; i++)
+    if (h[i] > 0) npos++;
+  const int sel = npos < m ? npos : m;
+  *nsel = sel;
+  if (sel == 0) return 0;
+  /* C = Z V Q3[:, largest theta first] diag(theta^-1/2) */
+  DEV_TRY(bdgd_scale_cols(dev, w->Ya, keep, keep - sel, sel, cplx, NULL, w->wH, 1, 1, w->T2s));
+  TRY(zgemm_small(w, 0, 0, keep, sel, keep, 1.0, w->V, keep, w->T2s, keep, 0.0, w->T1s, keep));
+  TRY(zgemm_small(w, 0, 0, k, sel, keep, 1.0, w->Z, k, w->T1s, keep, 0.0, w->C, k));
+  for (int j = 0; j < sel; j++) lam[j] = 1.0 / h[keep - 1 - j];
+  return 0;
+}
+
+/* ---- deflation of the Goldstone chain (real psi0) -------------------------- */
+static int deflate_block(ws_t *w, bdgd_ctx *dev, void *V, int q) {
+  if (!w->deflate || q <= 0) return 0;
+  const int S = (int)w->S, n = (int)w->n;
+  if (w->prec == BDGD_F32) {
+    const float *psi = (const float *)w->defl, *wv = psi + S;
+    float *coef = (float *)w->wtmp;
+    const float one = 1.f, zero = 0.f, c1 = (float)(-1.0 / w->wpsi);
+    BLAS_TRY(cublasSgemv(w->blas, CUBLAS_OP_T, S, q, &one, (const float *)V, n, wv, 1, &zero, coef, 1));
+    BLAS_TRY(cublasSger(w->blas, S, q, &c1, psi, 1, coef, 1, (float *)V, n));
+    BLAS_TRY(cublasSgemv(w->blas, CUBLAS_OP_T, S, q, &one, (const float *)V + S, n, psi, 1, &zero, coef, 1));
+    BLAS_TRY(cublasSger(w->blas, S, q, &c1, wv, 1, coef, 1, (float *)V + S, n));
+  } else {
+    const double *psi = w->defl, *wv = psi + S;
+    double *coef = w->wtmp;
+    const double one = 1.0, zero = 0.0, c1 = -1.0 / w->wpsi;
+    BLAS_TRY(cublasDgemv(w->blas, CUBLAS_OP_T, S, q, &one, (const double *)V, n, wv, 1, &zero, coef, 1));
+    BLAS_TRY(cublasDger(w->blas, S, q, &c1, psi, 1, coef, 1, (double *)V, n));
+    BLAS_TRY(cublasDgemv(w->blas, CUBLAS_OP_T, S, q, &one, (const double *)V + S, n, psi, 1, &zero, coef, 1));
+    BLAS_TRY(cublasDger(w->blas, S, q, &c1, wv, 1, coef, 1, (double *)V + S, n));
+  }
+  return 0;
+}
+
+/* w = M^-1 psi0 by conjugate gradients (FP64, on the device). */
+static int goldstone_setup(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int prec) {
+  const int S = (int)w->S;
+  double *x, *r, *p, *q, *psi;
+  TRY(dmalloc((void **)&x, 5 * (size_t)S * sizeof(double)));
+  r = x + S;
+  p = r + S;
+  q = p + S;
+  psi = q + S;
+  cudaStream_t st = stream_of(dev);
+  CUDA_TRY(cudaMemcpyAsync(psi, ctx->wf, (size_t)S * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(x, 0, (size_t)S * sizeof(double), st));
+  CUDA_TRY(cudaMemcpyAsync(r, psi, (size_t)S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(p, psi, (size_t)S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  double rr = 0, bn = 0;
+  BLAS_TRY(cublasSetPointerMode(w->blas, CUBLAS_POINTER_MODE_HOST));
+  BLAS_TRY(cublasDdot(w->blas, S, r, 1, r, 1, &rr));
+  bn = sqrt(rr);
+  for (int it = 0; it < 20000 && sqrt(rr) > 1e-13 * bn; it++) {
+    DEV_TRY(bdgd_apply(dev, BDGD_OP_M, BDGD_F64, p, (uint64_t)S, q, (uint64_t)S, 1));
+    double pq = 0;
+    BLAS_TRY(cublasDdot(w->blas, S, p, 1, q, 1, &pq));
+    const double al = rr / pq, nal = -al;
+    BLAS_TRY(cublasDaxpy(w->blas, S, &al, p, 1, x, 1));
+    BLAS_TRY(cublasDaxpy(w->blas, S, &nal, q, 1, r, 1));
+    double rn = 0;
+    BLAS_TRY(cublasDdot(w->blas, S, r, 1, r, 1, &rn));
+    const double be = rn / rr;
+    BLAS_TRY(cublasDscal(w->blas, S, &be, p, 1));
+    const double one = 1.0;
+    BLAS_TRY(cublasDaxpy(w->blas, S, &one, r, 1, p, 1));
+    rr = rn;
+  }
+  double wpsi = 0;
+  BLAS_TRY(cublasDdot(w->blas, S, x, 1, psi, 1, &wpsi));
+  w->wpsi = wpsi;
+  if (w->defl) cudaFree(w->defl);
+  w->defl = NULL;
+  TRY(dmalloc((void **)&w->defl, 2 * (size_t)S * sizeof(double)));
+  if (prec == BDGD_F32) {
+    DEV_TRY(bdgd_convert(dev, 1, psi, w->defl, (uint64_t)S));
+    DEV_TRY(bdgd_convert(dev, 1, x, (float *)w->defl + S, (uint64_t)S));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(w->defl, psi, (size_t)S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(w->defl + S, x, (size_t)S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  cudaFree(x);
+  w->deflate = 1;
+  return 0;
+}
+
+/* ---- convergence ------------------------------------------------------------- */
 static double now_s(void) {
   struct timespec t;
   clock_gettime(CLOCK_MONOTONIC, &t);
@@ -305,7 +497,6 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-/* ||A|| bound: max kinetic energy + largest local term (+ dipolar exchange). */
 static double anorm_estimate(const matmul_ctx_t *ctx) {
   double kin = 0.0;
   for (uint64_t d = 0; d < ctx->dim; d++) {
@@ -330,118 +521,223 @@ static double anorm_estimate(const matmul_ctx_t *ctx) {
   return kin + fmax(aK, aM);
 }
 
-/* Evaluate the convergence measure of the first nev columns; writes
- * res_host[nev]; returns the number converged. */
-static int check_convergence(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const void *X, const void *AX, double anorm,
-                             const double *lam_host, double *res_host, double *tres_host, int want_true) {
-  cudaStream_t st = (cudaStream_t)bdgd_stream(dev);
-  const int nev = (int)w->nev;
+/* Backward error of all m columns (back[]) and, with want_true, the true
+ * residual of the first nev (tres[]). */
+static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, double *back, double *tres,
+                   int want_true) {
+  const int m = (int)w->m, nev = (int)w->nev, K = w->K;
   double h[4 * 1024];
-  DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, w->m, X, AX, w->n, w->R, w->n, w->lam, w->work, w->norms,
-                        w->norms + w->kmax));
-  const int tr = want_true || bdg->criterion == BDG_CONV_TRUE_RESIDUAL;
-  if (tr) {
-    /* K (M v): M v is the lower half of AX */
-    const char *Mv = (const char *)AX + w->S * w->esz;
+  DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, (uint64_t)m, B(NB_X), B(NB_AX), w->n, NULL, w->n, w->lam_d,
+                        w->work, w->norms, w->norms + K, NULL));
+  if (want_true) {
+    const char *Mv = (const char *)B(NB_AX) + w->S * w->esz;
     DEV_TRY(bdgd_apply(dev, BDGD_OP_K, w->prec, Mv, w->n, w->TR, w->S, (uint64_t)nev));
-    DEV_TRY(bdgd_true_residual(dev, w->prec, w->cplx, w->S, (uint64_t)nev, w->TR, w->S, X, w->n, w->lam, w->work,
-                               w->norms + 2 * w->kmax, w->norms + 3 * w->kmax));
+    DEV_TRY(bdgd_true_residual(dev, w->prec, w->cplx, w->S, (uint64_t)nev, w->TR, w->S, B(NB_X), w->n, w->lam_d,
+                               w->work, w->norms + 2 * K, w->norms + 3 * K));
   }
-  CUDA_TRY(cudaMemcpyAsync(h, w->norms, 4 * w->kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  int nconv = 0;
-  for (int j = 0; j < nev; j++) {
-    const double rr = sqrt(h[j]), xx = sqrt(h[w->kmax + j]);
-    const double back = rr / ((anorm + fabs(lam_host[j])) * (xx > 0 ? xx : 1e-300));
-    double tres = NAN;
-    if (tr) {
-      const double tt = sqrt(h[2 * w->kmax + j]), vv = sqrt(h[3 * w->kmax + j]);
-      tres = tt / (vv > 0 ? vv : 1e-300);
+  TRY(host_vec(w, dev, w->norms, 4 * K, h));
+  for (int j = 0; j < m; j++) {
+    const double rr = sqrt(h[j]), xx = sqrt(h[K + j]);
+    back[j] = rr / ((anorm + fabs(lam[j])) * (xx > 0 ? xx : 1e-300));
+  }
+  if (want_true)
+    for (int j = 0; j < nev; j++) {
+      const double tt = sqrt(h[2 * K + j]), vv = sqrt(h[3 * K + j]);
+      tres[j] = tt / (vv > 0 ? vv : 1e-300);
     }
-    res_host[j] = (bdg->criterion == BDG_CONV_TRUE_RESIDUAL) ? tres : back;
-    if (tres_host) tres_host[j] = tres;
-    if (res_host[j] <= bdg->tol) nconv++;
-  }
-  return nconv;
+  return 0;
 }
 
-/* One full iLOBPCG run with blocks of the workspace precision, starting from
- * X in S0[:, 0:m].  Returns 0 or an error; leaves X, AX in S0/AS0. */
-static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, uint64_t maxit, double anorm, double *lam_host,
-                    uint64_t *iters, int *nconv_out, double *res_host) {
-  cudaStream_t st = (cudaStream_t)bdgd_stream(dev);
-  const uint64_t m = w->m, S = w->S;
-  const double drop = (w->prec == BDGD_F32) ? RR_DROP_F32 : RR_DROP_F64;
-  int rc, nsel = 0;
+/* ---- the iteration ----------------------------------------------------------- */
+typedef struct {
+  int criterion;
+  double tol;
+  uint64_t maxit;
+  double anorm;
+  int stop_backward_at_floor; /* FP32 phase: stop when backward errors reach this floor */
+  double floor;
+} loop_opts_t;
+
+/* X in B(NB_X) (m columns); runs RR on span X first.  On return lam holds the
+ * m Ritz values and res_nev the convergence measure of the nev wanted pairs. */
+static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, double *lam, double *res_nev,
+                    uint64_t *iters, int *nconv_out) {
+  cudaStream_t st = stream_of(dev);
+  const int m = (int)w->m, nev = (int)w->nev, K = w->K;
+  const size_t es = w->cplx ? 2 : 1;
+  const double drop = (w->prec == BDGD_F32) ? DROP_F32 : DROP_F64;
   bdg_solve_stats_t *ss = &bdg->stats;
-  /* AX = A X, Rayleigh-Ritz on span X */
+  int nsel = 0;
+  double back[1024], tres[1024];
+  int act[1024];
+  if (m > 1024) return -8;
+  /* AX, Rayleigh-Ritz on span X */
   cudaEventRecord(w->ev[0], st);
-  DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, w->S0, w->n, w->AS0, w->n, m));
+  TRY(deflate_block(w, dev, B(NB_X), m));
+  DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, B(NB_X), w->n, B(NB_AX), w->n, (uint64_t)m));
   cudaEventRecord(w->ev[1], st);
-  DEV_TRY(bdgd_gram(dev, w->prec, w->cplx, S, m, w->S0, w->n, w->AS0, w->n, w->gram));
-  if ((rc = rayleigh_ritz(w, dev, (int)m, (int)m, drop, lam_host, &nsel))) return rc;
-  if (nsel < (int)m) {
-    fprintf(stderr, "bdg_solve: initial block is not B-positive (%d of %lu positive-type)\n", nsel,
-            (unsigned long)m);
+  {
+    void *Sb[1] = {B(NB_X)}, *ASb[1] = {B(NB_AX)};
+    int kb[1] = {m};
+    TRY(rr_grams(w, dev, 1, Sb, ASb, kb));
+  }
+  TRY(rayleigh_ritz(w, dev, m, m, drop, lam, &nsel));
+  if (nsel < m) {
+    fprintf(stderr, "bdg_solve: initial block is not B-positive (%d of %d positive-type)\n", nsel, m);
     return -5;
   }
-  if ((rc = block_gemm(w, dev, w->S0, (int)m, w->C64, (int)m, (int)m, w->S1))) return rc;
-  if ((rc = block_gemm(w, dev, w->AS0, (int)m, w->C64, (int)m, (int)m, w->AS1))) return rc;
-  void *t;
-  t = w->S0; w->S0 = w->S1; w->S1 = t;
-  t = w->AS0; w->AS0 = w->AS1; w->AS1 = t;
-  CUDA_TRY(cudaMemcpyAsync(w->lam, lam_host, m * sizeof(double), cudaMemcpyHostToDevice, st));
+  TRY(bgemm(w, dev, B(NB_X), m, w->C, m, m, 1.0, 0.0, B(NB_XN)));
+  TRY(bgemm(w, dev, B(NB_AX), m, w->C, m, m, 1.0, 0.0, B(NB_AXN)));
+  swapb(w, NB_X, NB_XN);
+  swapb(w, NB_AX, NB_AXN);
+  CUDA_TRY(cudaMemcpyAsync(w->lam_d, lam, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, st));
+  cudaEventRecord(w->ev[2], st);
+  CUDA_TRY(cudaEventSynchronize(w->ev[2]));
   ss->ms_apply_A += ev_ms(w->ev[0], w->ev[1]);
-  ss->cols_apply_A += m;
-  int have_p = 0;
+  ss->cols_apply_A += (uint64_t)m;
+  w->p = 0;
   uint64_t it = 0;
   int nconv = 0;
+  const int want_true = (o->criterion == BDG_CONV_TRUE_RESIDUAL);
   for (;;) {
-    cudaEventRecord(w->ev[2], st);
-    nconv = check_convergence(w, dev, bdg, w->S0, w->AS0, anorm, lam_host, res_host, NULL, 0);
-    if (nconv < 0) return nconv;
     cudaEventRecord(w->ev[3], st);
-    if (nconv >= (int)w->nev || it >= maxit) break;
-    /* W = T R into the W slot, AW = A W */
-    void *W = col_ptr(w, w->S0, m), *AW = col_ptr(w, w->AS0, m);
-    DEV_TRY(bdgd_apply(dev, BDGD_OP_TLREP, w->prec, w->R, w->n, W, w->n, m));
+    TRY(measure(w, dev, o->anorm, lam, back, tres, want_true));
+    nconv = 0;
+    int na = 0;
+    double worst = 0.0;
+    for (int j = 0; j < nev; j++) {
+      res_nev[j] = want_true ? tres[j] : back[j];
+      if (res_nev[j] <= o->tol) nconv++;
+      else act[na++] = j;
+      worst = fmax(worst, back[j]);
+    }
+    for (int j = nev; j < m; j++)
+      if (back[j] > GUARD_LOCK) act[na++] = j;
+    if (nconv >= nev || it >= o->maxit) break;
+    if (o->stop_backward_at_floor && worst <= o->floor) break;
+    if (na == 0) break;
+    /* R = residual of the active columns (compact), W = T R */
+    CUDA_TRY(cudaMemcpyAsync(w->colmap, act, (size_t)na * sizeof(int), cudaMemcpyHostToDevice, st));
+    DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, (uint64_t)na, B(NB_X), B(NB_AX), w->n, B(NB_R), w->n,
+                          w->lam_d, w->work, w->norms, w->norms + K, w->colmap));
     cudaEventRecord(w->ev[4], st);
-    DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, W, w->n, AW, w->n, m));
+    DEV_TRY(bdgd_apply(dev, BDGD_OP_TLREP, w->prec, B(NB_R), w->n, B(NB_WT), w->n, (uint64_t)na));
     cudaEventRecord(w->ev[5], st);
-    const int k = have_p ? (int)(3 * m) : (int)(2 * m);
-    DEV_TRY(bdgd_gram(dev, w->prec, w->cplx, S, (uint64_t)k, w->S0, w->n, w->AS0, w->n, w->gram));
+    TRY(deflate_block(w, dev, B(NB_WT), na));
+    const int p = w->p;
+    /* P <- (P - X (X^H X)^+ X^H P) Z_P ; AP alike */
+    int pk = 0;
+    if (p > 0) {
+      bdgd_gram_task t[2];
+      t[0] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0);
+      t[1] = mk_task(w, B(NB_X), B(NB_P), w->n, m, p, 0, 0, m, 0, 0);
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 2, t, K, w->gout));
+      TRY(gram_pinv_apply(w, dev, w->gout, m, K, w->gout + (size_t)m * K * es, p, drop, w->Cs));
+      TRY(bgemm(w, dev, B(NB_X), m, w->Cs, m, p, -1.0, 1.0, B(NB_P)));
+      TRY(bgemm(w, dev, B(NB_AX), m, w->Cs, m, p, -1.0, 1.0, B(NB_AP)));
+      t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 0, 0, 0, 1, 0);
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
+      TRY(svqb(w, dev, w->gout, p, K, drop, w->Cs, &pk));
+      /* Cs holds Z_P (p x pk, leading dim p) */
+      TRY(bgemm(w, dev, B(NB_P), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T1)));
+      TRY(bgemm(w, dev, B(NB_AP), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T2)));
+      swapb(w, NB_P, NB_T1);
+      swapb(w, NB_AP, NB_T2);
+    }
+    /* W <- (Wt - Q (Q^H Q)^+ Q^H Wt) Z_W, Q = [X, P] */
+    const int q = m + pk;
+    {
+      bdgd_gram_task t[5];
+      int nt = 0;
+      t[nt++] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0);
+      t[nt++] = mk_task(w, B(NB_X), B(NB_WT), w->n, m, na, 0, 0, q, 0, 0);
+      if (pk > 0) {
+        t[nt++] = mk_task(w, B(NB_X), B(NB_P), w->n, m, pk, 0, 0, m, 0, 1);
+        t[nt++] = mk_task(w, B(NB_P), B(NB_P), w->n, pk, pk, 0, m, m, 1, 0);
+        t[nt++] = mk_task(w, B(NB_P), B(NB_WT), w->n, pk, na, 0, m, q, 0, 0);
+      }
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, nt, t, K, w->gout));
+      TRY(gram_pinv_apply(w, dev, w->gout, q, K, w->gout + (size_t)q * K * es, na, drop, w->Cs));
+      /* Cs: q x na (leading dim q) */
+      TRY(bgemm(w, dev, B(NB_X), m, w->Cs, q, na, -1.0, 1.0, B(NB_WT)));
+      if (pk > 0) TRY(bgemm(w, dev, B(NB_P), pk, w->Cs + (size_t)m * es, q, na, -1.0, 1.0, B(NB_WT)));
+      t[0] = mk_task(w, B(NB_WT), B(NB_WT), w->n, na, na, 0, 0, 0, 1, 0);
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
+    }
+    int wk = 0;
+    TRY(svqb(w, dev, w->gout, na, K, drop, w->Cs, &wk));
+    TRY(bgemm(w, dev, B(NB_WT), na, w->Cs, na, wk, 1.0, 0.0, B(NB_W)));
     cudaEventRecord(w->ev[6], st);
-    if ((rc = rayleigh_ritz(w, dev, k, (int)m, drop, lam_host, &nsel))) return rc;
+    DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, B(NB_W), w->n, B(NB_AW), w->n, (uint64_t)wk));
     cudaEventRecord(w->ev[7], st);
-    if (nsel < (int)m) {
-      fprintf(stderr, "bdg_solve: search space lost B-positivity (%d of %lu)\n", nsel, (unsigned long)m);
+    /* Rayleigh-Ritz on [X, P, W] */
+    const int k = m + pk + wk;
+    {
+      void *Sb[3] = {B(NB_X), B(NB_P), B(NB_W)}, *ASb[3] = {B(NB_AX), B(NB_AP), B(NB_AW)};
+      int kb[3] = {m, pk, wk};
+      TRY(rr_grams(w, dev, 3, Sb, ASb, kb));
+    }
+    cudaEventRecord(w->ev[8], st);
+    TRY(rayleigh_ritz(w, dev, k, m, drop, lam, &nsel));
+    if (nsel < m) {
+      fprintf(stderr, "bdg_solve: search space lost B-positivity (%d of %d)\n", nsel, m);
       return -6;
     }
-    /* X <- S C ; P <- S[:, m:k] C[m:k, :] (same for AS) */
-    const size_t cel = w->cplx ? 2 : 1;
-    const double *Cwp = w->C64 + m * cel;
-    if ((rc = block_gemm(w, dev, w->S0, k, w->C64, k, (int)m, w->S1))) return rc;
-    if ((rc = block_gemm(w, dev, W, k - (int)m, Cwp, k, (int)m, col_ptr(w, w->S1, 2 * m)))) return rc;
-    if ((rc = block_gemm(w, dev, w->AS0, k, w->C64, k, (int)m, w->AS1))) return rc;
-    if ((rc = block_gemm(w, dev, AW, k - (int)m, Cwp, k, (int)m, col_ptr(w, w->AS1, 2 * m)))) return rc;
-    cudaEventRecord(w->ev[8], st);
-    t = w->S0; w->S0 = w->S1; w->S1 = t;
-    t = w->AS0; w->AS0 = w->AS1; w->AS1 = t;
-    CUDA_TRY(cudaMemcpyAsync(w->lam, lam_host, m * sizeof(double), cudaMemcpyHostToDevice, st));
-    have_p = 1;
+    cudaEventRecord(w->ev[9], st);
+    /* X <- X Cx + P Cp + W Cw ; P <- P Cp + W Cw on the active columns */
+    const double *Cx = w->C, *Cp = w->C + (size_t)m * es, *Cw = w->C + (size_t)(m + pk) * es;
+    TRY(bgemm(w, dev, B(NB_X), m, Cx, k, m, 1.0, 0.0, B(NB_XN)));
+    TRY(bgemm(w, dev, B(NB_AX), m, Cx, k, m, 1.0, 0.0, B(NB_AXN)));
+    if (pk > 0) {
+      TRY(bgemm(w, dev, B(NB_P), pk, Cp, k, m, 1.0, 1.0, B(NB_XN)));
+      TRY(bgemm(w, dev, B(NB_AP), pk, Cp, k, m, 1.0, 1.0, B(NB_AXN)));
+    }
+    TRY(bgemm(w, dev, B(NB_W), wk, Cw, k, m, 1.0, 1.0, B(NB_XN)));
+    TRY(bgemm(w, dev, B(NB_AW), wk, Cw, k, m, 1.0, 1.0, B(NB_AXN)));
+    /* C restricted to the active columns and to the [P, W] rows */
+    CUDA_TRY(cudaMemcpyAsync(w->actcols, act, (size_t)na * sizeof(int), cudaMemcpyHostToDevice, st));
+    DEV_TRY(bdgd_gather_cols(dev, w->C + (size_t)m * es, k, pk + wk, w->actcols, na, w->cplx, w->T2s, pk + wk));
+    {
+      /* T2s (pk+wk x na) -> Cs to keep T2s free for the FP32 conversion in bgemm */
+      CUDA_TRY(cudaMemcpyAsync(w->Cs, w->T2s, (size_t)(pk + wk) * na * es * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+    }
+    if (pk > 0) {
+      TRY(bgemm(w, dev, B(NB_P), pk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_PN)));
+      TRY(bgemm(w, dev, B(NB_AP), pk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_APN)));
+      TRY(bgemm(w, dev, B(NB_W), wk, w->Cs + (size_t)pk * es, pk + wk, na, 1.0, 1.0, B(NB_PN)));
+      TRY(bgemm(w, dev, B(NB_AW), wk, w->Cs + (size_t)pk * es, pk + wk, na, 1.0, 1.0, B(NB_APN)));
+    } else {
+      TRY(bgemm(w, dev, B(NB_W), wk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_PN)));
+      TRY(bgemm(w, dev, B(NB_AW), wk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_APN)));
+    }
+    swapb(w, NB_X, NB_XN);
+    swapb(w, NB_AX, NB_AXN);
+    swapb(w, NB_P, NB_PN);
+    swapb(w, NB_AP, NB_APN);
+    w->p = (pk + wk > 0) ? na : 0;
+    CUDA_TRY(cudaMemcpyAsync(w->lam_d, lam, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, st));
+    cudaEventRecord(w->ev[10], st);
+    CUDA_TRY(cudaEventSynchronize(w->ev[10]));
+    ss->ms_residual += ev_ms(w->ev[3], w->ev[4]);
+    ss->ms_apply_T += ev_ms(w->ev[4], w->ev[5]);
+    ss->ms_gram += ev_ms(w->ev[5], w->ev[6]) + ev_ms(w->ev[7], w->ev[8]);
+    ss->ms_apply_A += ev_ms(w->ev[6], w->ev[7]);
+    ss->ms_small_dense += ev_ms(w->ev[8], w->ev[9]);
+    ss->ms_update += ev_ms(w->ev[9], w->ev[10]);
+    ss->cols_apply_A += (uint64_t)wk;
+    ss->cols_apply_T += (uint64_t)na;
     it++;
-    CUDA_TRY(cudaEventSynchronize(w->ev[8]));
-    ss->ms_residual += ev_ms(w->ev[2], w->ev[3]);
-    ss->ms_apply_T += ev_ms(w->ev[3], w->ev[4]);
-    ss->ms_apply_A += ev_ms(w->ev[4], w->ev[5]);
-    ss->ms_gram += ev_ms(w->ev[5], w->ev[6]);
-    ss->ms_small_dense += ev_ms(w->ev[6], w->ev[7]);
-    ss->ms_update += ev_ms(w->ev[7], w->ev[8]);
-    ss->cols_apply_A += m;
-    ss->cols_apply_T += m;
   }
   *iters = it;
   *nconv_out = nconv;
+  (void)es;
+  return 0;
+}
+
+/* copy the FP32 block X (and nothing else) into a fresh FP64 workspace */
+static int to_f64(ws_t *w32, ws_t *w64, bdgd_ctx *dev) {
+  DEV_TRY(bdgd_convert(dev, 0, w32->blk[NB_X], w64->blk[NB_X], w32->n * w32->m * (w32->cplx ? 2 : 1)));
   return 0;
 }
 
@@ -451,14 +747,13 @@ static int solve_gpu(bdg_t *bdg) {
   const int cplx = bdg->complex_psi0;
   const uint64_t S = ctx->size, n = 2 * S, m = bdg->sizeSub, nev = bdg->nev;
   memset(&bdg->stats, 0, sizeof bdg->stats);
-  if (nev == 0 || m < nev) {
-    fprintf(stderr, "bdg_solve: need 0 < nev <= sizeSub\n");
+  if (nev == 0 || m < nev || m > 1000) {
+    fprintf(stderr, "bdg_solve: need 0 < nev <= sizeSub <= 1000\n");
     return -7;
   }
   safe_free((void **)&bdg->eigvals);
   safe_free(&bdg->modes_u);
   safe_free(&bdg->modes_v);
-  /* mirror every operator field on the device */
   int rc = bdg_ctx_sync_device(ctx, BDGD_OP_LREP);
   if (!rc) rc = bdg_ctx_sync_device(ctx, BDGD_OP_TLREP);
   if (rc) {
@@ -466,53 +761,82 @@ static int solve_gpu(bdg_t *bdg) {
     return rc;
   }
   bdgd_ctx *dev = ctx->dev;
-  cudaStream_t st = (cudaStream_t)bdgd_stream(dev);
-  if (!bdg->solver_ws) bdg->solver_ws = xcalloc(1, sizeof(ws_t));
-  ws_t *w = (ws_t *)bdg->solver_ws;
-  const int prec = (bdg->precision == BDG_PREC_MIXED) ? BDGD_F32 : BDGD_F64;
-  if ((rc = ws_setup(w, dev, S, m, nev, cplx, prec))) return rc;
-  /* initial block on the host, then to the device */
+  cudaStream_t st = stream_of(dev);
+  if (!bdg->solver_ws) bdg->solver_ws = xcalloc(2, sizeof(ws_t));
+  ws_t *wsp = (ws_t *)bdg->solver_ws; /* [0] FP64 workspace, [1] FP32 workspace */
+  const int mixed = (bdg->precision == BDG_PREC_MIXED);
+  ws_t *w = mixed ? &wsp[1] : &wsp[0];
+  if ((rc = ws_setup(w, dev, S, m, nev, cplx, mixed ? BDGD_F32 : BDGD_F64))) return rc;
+  const int deflate = bdg->deflate && !cplx && ctx->wf;
+  w->deflate = 0;
+  if (deflate && (rc = goldstone_setup(w, dev, ctx, w->prec))) return rc;
+  /* initial block: host fill, upload (converted for FP32) */
   const size_t hesz = cplx ? sizeof(c64) : sizeof(f64);
   void *X0 = xcalloc(n * m, hesz);
   bdg_fill_initial_block(bdg, X0);
-  if (prec == BDGD_F32) {
+  if (mixed) {
     void *tmp = NULL;
     if ((rc = dmalloc(&tmp, n * m * hesz))) return rc;
     CUDA_TRY(cudaMemcpyAsync(tmp, X0, n * m * hesz, cudaMemcpyHostToDevice, st));
-    DEV_TRY(bdgd_convert(dev, 1, tmp, w->S0, n * m * (cplx ? 2 : 1)));
+    DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
     CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(tmp);
   } else {
-    CUDA_TRY(cudaMemcpyAsync(w->S0, X0, n * m * hesz, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, n * m * hesz, cudaMemcpyHostToDevice, st));
   }
+  free(X0);
   const double anorm = anorm_estimate(ctx);
   double *lam = xcalloc(3 * m, sizeof(double));
   double *res = xcalloc(nev, sizeof(double));
-  uint64_t iters = 0;
+  uint64_t iters = 0, iters2 = 0;
   int nconv = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
-  rc = run_loop(w, dev, bdg, bdg->maxIter, anorm, lam, &iters, &nconv, res);
+  loop_opts_t o;
+  memset(&o, 0, sizeof o);
+  o.criterion = bdg->criterion;
+  o.tol = bdg->tol;
+  o.maxit = bdg->maxIter;
+  o.anorm = anorm;
+  if (mixed) {
+    loop_opts_t o32 = o;
+    o32.criterion = BDG_CONV_BACKWARD;
+    o32.tol = fmax(bdg->tol, MIXED_SWITCH);
+    o32.stop_backward_at_floor = 1;
+    o32.floor = MIXED_SWITCH;
+    rc = run_loop(w, dev, bdg, &o32, lam, res, &iters, &nconv);
+    if (!rc) {
+      ws_t *w64 = &wsp[0];
+      if ((rc = ws_setup(w64, dev, S, m, nev, cplx, BDGD_F64))) return rc;
+      w64->deflate = 0;
+      if (deflate && (rc = goldstone_setup(w64, dev, ctx, BDGD_F64))) return rc;
+      if ((rc = to_f64(w, w64, dev))) return rc;
+      w = w64;
+      o.maxit = bdg->maxIter > iters ? bdg->maxIter - iters : 0;
+      rc = run_loop(w, dev, bdg, &o, lam, res, &iters2, &nconv);
+      bdg->stats.refine_iterations = iters2;
+    }
+  } else {
+    rc = run_loop(w, dev, bdg, &o, lam, res, &iters, &nconv);
+  }
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);
   bdg->stats.seconds_device = 1e-3 * ev_ms(e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  bdg->stats.iterations = iters;
+  bdg->stats.iterations = iters + iters2;
   if (rc) {
     bdg->stats.status = rc;
-    free(X0);
     free(lam);
     free(res);
     return rc;
   }
-  /* final true residual of the wanted pairs (reported in the stats) */
-  double *tres = xcalloc(nev, sizeof(double));
+  /* final measures of the wanted pairs */
   {
-    double *tmp = xcalloc(nev, sizeof(double));
-    check_convergence(w, dev, bdg, w->S0, w->AS0, anorm, lam, tmp, tres, 1);
+    double back[1024], tres[1024];
+    TRY(measure(w, dev, anorm, lam, back, tres, 1));
     double mx = 0.0, mt = 0.0;
     for (uint64_t j = 0; j < nev; j++) {
       mx = fmax(mx, res[j]);
@@ -520,25 +844,14 @@ static int solve_gpu(bdg_t *bdg) {
     }
     bdg->stats.max_residual = mx;
     bdg->stats.max_true_residual = mt;
-    free(tmp);
   }
-  /* results: eigenvalues, modes, full block */
   bdg->converged = (uint64_t)nconv;
   bdg->eigvals = xcalloc(nev, sizeof(f64));
   memcpy(bdg->eigvals, lam, nev * sizeof(f64));
   safe_free(&bdg->block);
   bdg->block = xcalloc(n * m, hesz);
-  if (prec == BDGD_F32) {
-    void *tmp = NULL;
-    if ((rc = dmalloc(&tmp, n * m * hesz))) return rc;
-    DEV_TRY(bdgd_convert(dev, 0, w->S0, tmp, n * m * (cplx ? 2 : 1)));
-    CUDA_TRY(cudaMemcpyAsync(bdg->block, tmp, n * m * hesz, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(tmp);
-  } else {
-    CUDA_TRY(cudaMemcpyAsync(bdg->block, w->S0, n * m * hesz, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-  }
+  CUDA_TRY(cudaMemcpyAsync(bdg->block, w->blk[NB_X], n * m * hesz, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
   char *mu = xcalloc(S * nev, hesz), *mv = xcalloc(S * nev, hesz);
   for (uint64_t j = 0; j < nev; j++) {
     memcpy(mu + j * S * hesz, (char *)bdg->block + j * n * hesz, S * hesz);
@@ -546,10 +859,8 @@ static int solve_gpu(bdg_t *bdg) {
   }
   bdg->modes_u = mu;
   bdg->modes_v = mv;
-  free(X0);
   free(lam);
   free(res);
-  free(tres);
   bdg->stats.seconds_total = now_s() - t0;
   return 0;
 }

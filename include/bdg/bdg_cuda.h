@@ -103,6 +103,22 @@ int bdgd_gram(bdgd_ctx *ctx, int prec, int cplx, uint64_t half, uint64_t k,
               const void *d_S, uint64_t lds, const void *d_AS, uint64_t ldas,
               double *d_out);
 
+/* General Gram task list: task t computes C = A^H B (rows x ka by rows x kb,
+ * column-major, leading dimensions in elements) into output matrix `out`
+ * (ldo x ldo, column-major, FP64 or interleaved complex) at rows i0.., columns
+ * j0...  `sym` marks a diagonal block A == B (upper tiles computed, lower
+ * filled by symmetry); `mirror` also writes C^H at (j0.., i0..).  Up to 48
+ * tasks per call; all tasks in one launch. */
+typedef struct {
+  const void *a;
+  const void *b;
+  uint64_t lda, ldb, rows;
+  int ka, kb, out, i0, j0, sym, mirror;
+} bdgd_gram_task;
+
+int bdgd_gram_tasks(bdgd_ctx *ctx, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
+                    double *d_out);
+
 #ifdef __cplusplus
 }
 #endif

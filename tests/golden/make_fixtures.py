@@ -1,0 +1,52 @@
+"""Generate the ground-state fixtures of the GPU parity tests and of the
+32^3 benchmark config (committed as .npz next to this script).
+
+Each psi0 comes from the oracle's split-step imaginary-time propagation
+(oracle/bdg_oracle.py: itp_ground_state): unit Gaussian start, dt = 1e-3,
+stopped when the per-step change of mu = <psi|H|psi> is below 1e-12,
+normalised to sum |psi|^2 dV = 1 on the grid x_i = (i - N/2) L / N.  The
+ITP state carries the O(dt^2) splitting error of the time stepping
+(||H psi - mu psi|| ~ 1e-3 here); it is then polished by bordered Newton
+steps (newton_polish) to the exact discrete stationary state, so that
+K psi0 = 0 to ~1e-14 and the Goldstone mode is exact.
+
+    python tests/golden/make_fixtures.py [name ...]
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle import bdg_oracle as O  # noqa: E402
+
+# name: (N, L, trap frequencies (x, y, z), g, g_dd, cutoff radius)
+PROBLEMS = {
+    # small dipolar trap for solver parity tests
+    "gs16": ([16, 16, 16], [8.0, 8.0, 8.0], (1.0, 1.0, 2.0), 100.0, 40.0, 4.0),
+    # dipolar trap of the 32^3 benchmark config: box [-8, 8)^3, lambda = 2,
+    # g = 1000, eps_dd = 0.5, dipoles along z, R_c = 8
+    "c1_32": ([32, 32, 32], [16.0, 16.0, 16.0], (1.0, 1.0, 2.0), 1000.0, 500.0, 8.0),
+}
+
+
+def make(name):
+    N, L, om, g, gdd, rc = PROBLEMS[name]
+    t = time.time()
+    psi, mu_itp, steps = O.itp_ground_state(N, L, om, g, gdd, (0.0, 0.0, 1.0), rc, dt=1e-3, tol=1e-12)
+    psi, mu, res = O.newton_polish(N, L, om, g, gdd, psi, rc)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), psi=psi, mu=mu, mu_itp=mu_itp, steps=steps,
+                        stationarity=res, N=N, L=L, omegas=om, g=g, gdd=gdd, rc=rc)
+    print(name, "mu_itp", mu_itp, "mu", mu, "|H psi - mu psi|", res, "steps", steps, "%.1fs" % (time.time() - t))
+
+
+def load(name):
+    d = np.load(os.path.join(HERE, f"{name}.npz"))
+    return {k: d[k] for k in d.files}
+
+
+if __name__ == "__main__":
+    for nm in (sys.argv[1:] or list(PROBLEMS)):
+        make(nm)

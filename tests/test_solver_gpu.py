@@ -1,0 +1,163 @@
+"""GPU iLOBPCG through the public C API (bdg_solve), against analytic
+spectra (the reference's solver tests restated) and against the CPU oracle
+solve on the same psi0, seed and initial block.
+
+Parity bar (FP64): eigenvalues within 1e-9 relative of the oracle, true BdG
+residual ||K M v - w^2 v||/||v|| <= tol, eigenvector subspace angles <= 1e-6.
+"""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import bdg_oracle as O
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+import make_fixtures as FX  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _uniform_1d(B, cplx):
+    p = B.Problem(1, [64], [2 * math.pi], cplx)
+    p.set_system()
+    p.set_solver_params(4, 10, 200, 1e-4)
+    p.set_wavefunction(np.ones(64))
+    p.set_local_interactions(lambda n: 1.0 * n, lambda n: 1.0 * n)
+    p.set_mu(1.0)
+    return p
+
+
+def test_bdg_1d_uniform_spectrum(bdg):
+    """tests/test_bdg_1d_uniform.c:60-140: two eigenvalues at sqrt(1.25) and
+    at least one at sqrt(8) within 1% (planewave init, nev 4, sizeSub 10)."""
+    p = _uniform_1d(bdg, False)
+    assert p.solve() == 0
+    assert p.converged() >= 4
+    ev = p.eigenvalues()
+    E1, E2 = math.sqrt(1.25), math.sqrt(8.0)
+    assert np.sum(np.abs(ev - E1) < 0.01 * E1) == 2, ev
+    assert np.sum(np.abs(ev - E2) < 0.01 * E2) >= 1, ev
+
+
+def test_bdg_1d_uniform_z_matches_d(bdg):
+    """tests/test_bdg_1d_uniform.c:142-230: complex path agrees (1e-4)."""
+    pd = _uniform_1d(bdg, False)
+    pz = _uniform_1d(bdg, True)
+    assert pd.solve() == 0 and pz.solve() == 0
+    assert pd.converged() >= 4 and pz.converged() >= 4
+    E1 = math.sqrt(1.25)
+    d = pd.eigenvalues()
+    z = pz.eigenvalues()
+    assert abs(d[np.argmin(np.abs(d - E1))] - z[np.argmin(np.abs(z - E1))]) < 1e-4
+
+
+@pytest.mark.parametrize("N", [32, 64])
+def test_bdg_3d_harmonic(N, bdg):
+    """tests/test_bdg_3d_harmonic.c:51-108 (64^3, L=10, nev 10, sizeSub 20,
+    tol 1e-4, no interactions): Goldstone mode at 0 +- 0.1 and the analytic
+    isotropic-oscillator excitations 1 (x3) and 2 (x6) within 5%.  (The
+    reference test asserts 1.0 for all nine excited values, which the
+    analytic spectrum omega = n does not satisfy for n = 2.)"""
+    p = bdg.Problem(3, [N] * 3, [10.0] * 3)
+    p.set_system()
+    c = (np.arange(N) - N / 2) * 10.0 / N
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    p.set_trap((0.5 * (X ** 2 + Y ** 2 + Z ** 2)).reshape(-1))
+    p.set_mu(1.5)
+    p.set_solver_params(10, 20, 500, 1e-4)
+    assert p.solve() == 0
+    assert p.converged() >= 10
+    ev = p.eigenvalues()
+    assert abs(ev[0]) < 0.1
+    assert np.all(np.abs(ev[1:4] - 1.0) < 0.05), ev
+    assert np.all(np.abs(ev[4:10] - 2.0) < 0.10), ev
+
+
+def _dipolar_problem(B, name, cplx=False, phase=0.0):
+    fx = FX.load(name)
+    N = [int(v) for v in fx["N"]]
+    L = [float(v) for v in fx["L"]]
+    om = [float(v) for v in fx["omegas"]]
+    g, gdd, rc, mu = float(fx["g"]), float(fx["gdd"]), float(fx["rc"]), float(fx["mu"])
+    psi = fx["psi"]
+    if cplx:
+        psi = psi * np.exp(1j * phase)
+    oc = O.build_problem(N, L, om, g, gdd, psi, mu, Rc=rc, complex_psi0=cplx)
+    p = B.Problem(3, N, L, cplx)
+    p.set_system()
+    p.set_trap(O.harmonic_trap(oc, om))
+    p.set_wavefunction(psi)
+    p.set_local_interactions(lambda n: g * n, lambda n: g * n)
+    p.set_dipolar(gdd, [0.0, 0.0, 1.0], rc)
+    p.set_mu(mu)
+    return oc, p
+
+
+def _subspace_angle(A, Bm):
+    qa, _ = np.linalg.qr(A.T)
+    qb, _ = np.linalg.qr(Bm.T)
+    s = np.linalg.svd(qa.conj().T @ qb, compute_uv=False)
+    return float(np.arccos(np.clip(np.min(s), -1.0, 1.0)))
+
+
+def test_setup_matches_oracle(bdg):
+    """Setup chain (trap, wf, interactions, dipolar kernel + GPU mean field,
+    mu) gives the oracle's local terms and preconditioner scalings."""
+    oc, p = _dipolar_problem(bdg, "gs16")
+    K, M = p.local_terms()
+    scale = np.max(np.abs(oc.localTermK))
+    assert np.max(np.abs(K - oc.localTermK)) < 1e-12 * scale
+    assert np.max(np.abs(M - oc.localTermM)) < 1e-12 * scale
+    pK = np.ctypeslib.as_array(p.ctx.precond_sqrtK, shape=(oc.size,))
+    assert np.max(np.abs(pK - oc.precond_sqrtK)) < 1e-12 * np.max(pK)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_solver_parity_with_oracle(precision, bdg):
+    """16^3 dipolar trap, nev 4, sizeSub 8, Goldstone deflation, true-residual
+    criterion tol 1e-8, same B-positive Gaussian block (seed 0) on both
+    sides.  FP64 and mixed FP32/FP64 must meet the FP64 bar."""
+    oc, p = _dipolar_problem(bdg, "gs16")
+    nev, m, tol = 4, 8, 1e-8
+    X0 = O.gaussian_block_bpositive(oc, m, 0)
+    proj, _ = O.goldstone_projector(oc)
+    ref = O.ilobpcg(oc, X0, nev, 400, tol, proj=proj, criterion=O.CONV_TRUE_RESIDUAL)
+    assert ref.converged >= nev
+    p.set_solver_params(nev, m, 400, tol)
+    p.set_initial_block(X0)
+    p.set_goldstone_deflation(True)
+    p.set_convergence(bdg.CONV_TRUE_RESIDUAL)
+    p.set_precision(precision)
+    assert p.solve() == 0
+    assert p.converged() >= nev
+    ev = p.eigenvalues()
+    rel = np.abs(ev - ref.eigvals[:nev]) / np.abs(ref.eigvals[:nev])
+    assert np.all(rel < 1e-9), (ev, ref.eigvals[:nev], rel)
+    st = p.stats()
+    assert st["max_true_residual"] <= tol
+    X = p.block()[:nev]
+    # true residual recomputed on the oracle from the returned modes
+    AX = O.matmulLrep(oc, X)
+    tres = O.true_residual(oc, X, AX, ev, nev)
+    assert np.all(tres <= 2 * tol), tres
+    # eigenvector subspace of the well-separated pairs
+    assert _subspace_angle(X, ref.X[:nev]) < 1e-6
+
+
+def test_complex_path_matches_real(bdg):
+    """A globally rotated psi0 = e^{i phi} psi_real is the same physics: the
+    complex (_z) path must reproduce the real (_d) eigenvalues (1e-9)."""
+    oc, pd = _dipolar_problem(bdg, "gs16")
+    _, pz = _dipolar_problem(bdg, "gs16", cplx=True, phase=0.7)
+    nev, m, tol = 4, 8, 1e-9
+    for p in (pd, pz):
+        p.set_solver_params(nev, m, 400, tol)
+        p.set_init_mode(bdg.INIT_PLANEWAVE)
+    assert pd.solve() == 0 and pz.solve() == 0
+    d, z = pd.eigenvalues(), pz.eigenvalues()
+    # skip the Goldstone pair (near 0) and compare the rest
+    sel = d > 1e-2
+    assert np.all(np.abs(d[sel] - z[sel]) < 1e-9 * np.abs(d[sel]) + 1e-9), (d, z)
