@@ -304,3 +304,23 @@ void bdg_set_local_interactions_grid(bdg_t *bdg, const double *uK, const double 
   }
   bdg->state |= BDG_HAS_INTERACTIONS;
 }
+
+/* ---- ground-state producer (no reference counterpart) ---------------------- */
+int bdg_ground_state(uint64_t dim, const uint64_t *N, const double *L, const double *V, double g, double g_ddi,
+                     const double *dipole_dir, double cutoff_radius, double dt, double tol, uint64_t max_steps,
+                     int newton_steps, double *psi_inout, double *mu_out, uint64_t *steps_out,
+                     double *stationarity_out) {
+  matmul_ctx_t *ctx = matmul_ctx_alloc(dim, N, L);
+  matmul_ctx_set_system(ctx, 0);
+  if (g_ddi != 0.0 && dim == 3) dipolar_set_kernel(ctx, g_ddi, dipole_dir, cutoff_radius);
+  int rc = bdg_ctx_sync_device(ctx, BDGD_OP_KINETIC);
+  if (!rc && ctx->longRngInt) rc = bdgd_set_dipolar(ctx->dev, ctx->longRngInt, g_ddi, 1);
+  int steps = 0;
+  if (!rc)
+    rc = bdgd_ground_state(ctx->dev, V, g, dt, tol, (int)max_steps, newton_steps, psi_inout, mu_out, &steps,
+                           stationarity_out);
+  if (rc) fprintf(stderr, "bdg_ground_state: %s\n", bdgd_last_error());
+  if (steps_out) *steps_out = (uint64_t)steps;
+  matmul_ctx_free(&ctx);
+  return rc;
+}

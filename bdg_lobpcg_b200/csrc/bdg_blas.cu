@@ -260,19 +260,24 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
   if (prec == BDGD_F32) {
     if (cplx) {
       BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_gram_tasks<float, true><<<grid, 128, sm, c->stream>>>(g);
     } else {
+      bdgd_count_launch();
       k_gram_tasks<float, false><<<grid, 128, sm, c->stream>>>(g);
     }
   } else {
     if (cplx) {
       BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_gram_tasks<double, true><<<grid, 128, sm, c->stream>>>(g);
     } else {
+      bdgd_count_launch();
       k_gram_tasks<double, false><<<grid, 128, sm, c->stream>>>(g);
     }
   }
   BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
   k_gram_tasks_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, cplx, ldo, d_out);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -395,6 +400,7 @@ extern "C" int bdgd_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half, uin
   const int nb = norm_blocks(2 * half_el);
   double *pr = d_work, *px = d_work + (long long)nb * ncol;
   dim3 grid(nb, (unsigned)ncol);
+  bdgd_count_launch();
   if (prec == BDGD_F32)
     k_residual<float><<<grid, 256, 0, c->stream>>>((const float *)d_X, (const float *)d_AX, (long long)ld * es,
                                                    (float *)d_R, (long long)ldr * es, d_lam, half_el, pr, px, d_colmap);
@@ -402,7 +408,9 @@ extern "C" int bdgd_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half, uin
     k_residual<double><<<grid, 256, 0, c->stream>>>((const double *)d_X, (const double *)d_AX, (long long)ld * es,
                                                     (double *)d_R, (long long)ldr * es, d_lam, half_el, pr, px, d_colmap);
   BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(pr, nb, (int)ncol, d_rr);
+  bdgd_count_launch();
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(px, nb, (int)ncol, d_xx);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -416,6 +424,7 @@ extern "C" int bdgd_true_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half
   const int nb = norm_blocks(half_el);
   double *pt = d_work, *pv = d_work + (long long)nb * ncol;
   dim3 grid(nb, (unsigned)ncol);
+  bdgd_count_launch();
   if (prec == BDGD_F32)
     k_true_residual<float><<<grid, 256, 0, c->stream>>>((const float *)d_KMv, (long long)ldk * es,
                                                         (const float *)d_X, (long long)ld * es, d_lam, half_el, pt,
@@ -425,7 +434,9 @@ extern "C" int bdgd_true_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half
                                                          (const double *)d_X, (long long)ld * es, d_lam, half_el, pt,
                                                          pv);
   BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(pt, nb, (int)ncol, d_tt);
+  bdgd_count_launch();
   k_sum_parts<<<((int)ncol + 127) / 128, 128, 0, c->stream>>>(pv, nb, (int)ncol, d_vv);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -447,6 +458,7 @@ extern "C" int bdgd_convert(bdgd_ctx *c, int to_f32, const void *src, void *dst,
   long long nb = ((long long)n_scalars + 255) / 256;
   if (nb > 8192) nb = 8192;
   if (nb < 1) nb = 1;
+  bdgd_count_launch();
   if (to_f32)
     k_d2f<<<(int)nb, 256, 0, c->stream>>>((const double *)src, (float *)dst, (long long)n_scalars);
   else
@@ -554,6 +566,7 @@ static int grid_for(long long n) {
 
 extern "C" int bdgd_rr_prepare(bdgd_ctx *c, const double *G, const double *Ga_in, const double *Guv, int k, int ldo,
                                int cplx, double *Gs, double *Gb, double *Ga, double *d) {
+  bdgd_count_launch();
   k_rr_prepare<<<grid_for((long long)k * k), 256, 0, c->stream>>>(G, Ga_in, Guv, k, ldo, cplx, Gs, Gb, Ga, d);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -561,6 +574,7 @@ extern "C" int bdgd_rr_prepare(bdgd_ctx *c, const double *G, const double *Ga_in
 
 extern "C" int bdgd_scale_cols(bdgd_ctx *c, const double *In, int rows, int col0, int ncols, int cplx,
                                const double *rowscale, const double *colval, int invsqrt, int reverse, double *Out) {
+  bdgd_count_launch();
   k_scale_cols<<<grid_for((long long)rows * ncols), 256, 0, c->stream>>>(In, rows, col0, ncols, cplx, rowscale,
                                                                           colval, invsqrt, reverse, Out);
   BDGD_CK(cudaGetLastError());
@@ -568,12 +582,14 @@ extern "C" int bdgd_scale_cols(bdgd_ctx *c, const double *In, int rows, int col0
 }
 
 extern "C" int bdgd_hermitize(bdgd_ctx *c, double *A, int k, int cplx) {
+  bdgd_count_launch();
   k_hermitize<<<grid_for((long long)k * k), 256, 0, c->stream>>>(A, k, cplx);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
 
 extern "C" int bdgd_clamp(bdgd_ctx *c, double *w, int n, double floor_rel) {
+  bdgd_count_launch();
   k_clamp<<<1, 256, 0, c->stream>>>(w, n, floor_rel);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -586,6 +602,7 @@ __global__ void k_vec_pow(const double *__restrict__ in, int n, double e, double
 }
 
 extern "C" int bdgd_vec_pow(bdgd_ctx *c, const double *in, int n, double e, double *out) {
+  bdgd_count_launch();
   k_vec_pow<<<(n + 255) / 256, 256, 0, c->stream>>>(in, n, e, out);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
@@ -604,6 +621,7 @@ __global__ void k_gather_cols(const double *__restrict__ In, int ldi, int rows, 
 
 extern "C" int bdgd_gather_cols(bdgd_ctx *c, const double *In, int ldi, int rows, const int *d_cols, int ncols,
                                 int cplx, double *Out, int ldo) {
+  bdgd_count_launch();
   k_gather_cols<<<grid_for((long long)rows * ncols), 256, 0, c->stream>>>(In, ldi, rows, d_cols, ncols, cplx, Out,
                                                                            ldo);
   BDGD_CK(cudaGetLastError());

@@ -36,6 +36,7 @@ struct FieldsDev {
   double g_ddi;
   double mu;
   double inv_size;
+  double kin_dt;  // exp(-kin_dt k^2) multiplier of the imaginary-time step
 };
 
 struct bdgd_ctx {
@@ -68,7 +69,13 @@ struct bdgd_ctx {
   double *gram_part;
   size_t gram_part_bytes;
   size_t spec_cap;  // max scratch bytes per apply chunk
+  double kin_dt;
 };
+
+int bdgd_run_internal(bdgd_ctx *c, int kind, const void *d_x, long long ldx, void *d_y, long long ldy, int ncol);
+
+// kernel launch counter (defined in bdg_ops.cu)
+void bdgd_count_launch(void);
 
 // error helpers (defined in bdg_ops.cu)
 void bdgd_set_error(const char *fmt, ...);

@@ -48,6 +48,10 @@ int bdgd_check(cudaError_t e, const char *what) {
 
 extern "C" const char *bdgd_last_error(void) { return g_err; }
 
+static unsigned long long g_launches = 0;
+void bdgd_count_launch(void) { __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+extern "C" unsigned long long bdgd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
 extern "C" int bdgd_device_count(void) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess) {
@@ -292,8 +296,8 @@ __device__ C *smem_fft(C *a, C *b, int nlines, int ls, const AxisDev &ax, int sg
 // ---------------------------------------------------------------------------
 // operator programs
 // ---------------------------------------------------------------------------
-enum { PRE_NONE = 0, PRE_PK, PRE_PM, PRE_CONJWF, PRE_DENS };
-enum { MUL_KIN = 0, MUL_DIP, MUL_PRE, MUL_ONE };
+enum { PRE_NONE = 0, PRE_PK, PRE_PM, PRE_CONJWF, PRE_DENS, PRE_XDENS };
+enum { MUL_KIN = 0, MUL_DIP, MUL_PRE, MUL_ONE, MUL_EXPKIN };
 enum { POST_RAW = 0, POST_K, POST_M, POST_TK, POST_TM, POST_DIPCONV, POST_PHI };
 
 struct Prog {
@@ -329,6 +333,10 @@ static Prog make_prog(int op, int dipolar) {
         p.nf[h] = 1; p.pre[h][0] = PRE_CONJWF; p.mul[h][0] = MUL_DIP; p.post[h] = POST_DIPCONV; break;
       case 100:  // dipolar mean field of |psi0|^2
         p.nf[h] = 1; p.pre[h][0] = PRE_DENS; p.mul[h][0] = MUL_DIP; p.post[h] = POST_PHI; break;
+      case 101:  // exp(-kin_dt k^2) propagator (imaginary-time kinetic half step)
+        p.nf[h] = 1; p.pre[h][0] = PRE_NONE; p.mul[h][0] = MUL_EXPKIN; p.post[h] = POST_RAW; break;
+      case 102:  // dipolar mean field of the input field |x|^2
+        p.nf[h] = 1; p.pre[h][0] = PRE_XDENS; p.mul[h][0] = MUL_DIP; p.post[h] = POST_PHI; break;
     }
   };
   if (op == BDGD_OP_LREP) {
@@ -360,6 +368,7 @@ __device__ __forceinline__ double kmult(const GeoDev &g, const FieldsDev &f, int
   if (g.dim > 1) k2 += __ldg(g.kx2[1] + iy);
   if (g.dim > 2) k2 += __ldg(g.kx2[2] + iz);
   if (kind == MUL_KIN) return k2 * (0.5 * f.inv_size);
+  if (kind == MUL_EXPKIN) return exp(-f.kin_dt * k2) * f.inv_size;
   double d = f.mu + 0.5 * k2;
   if (fabs(d) < 1e-8) d = 1e-8;
   return f.inv_size / d;
@@ -401,6 +410,7 @@ __device__ __forceinline__ typename El<T, CPLX>::C prologue(const FieldsDev &f, 
         T a = hypot(z.x, z.y);
         return cmk<C>(a * a, 0.0);
       }
+      case PRE_XDENS: return cmk<C>(x.x * x.x + x.y * x.y, 0.0);
       default: return x;
     }
   } else {
@@ -412,6 +422,7 @@ __device__ __forceinline__ typename El<T, CPLX>::C prologue(const FieldsDev &f, 
         T a = fabs(w[r]);
         return cmk<C>(a * a, 0.0);
       }
+      case PRE_XDENS: return cmk<C>(x * x, 0.0);
       default: return cmk<C>(x, 0.0);
     }
   }
@@ -908,6 +919,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
   fd.g_ddi = c->g_ddi;
   fd.mu = c->mu;
   fd.inv_size = 1.0 / (double)c->S;
+  fd.kin_dt = c->kin_dt;
   const GeoDev &g = c->geo;
   const int Nx = c->N[0];
   const int rpb = rows_per_block(Nx);
@@ -918,6 +930,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
     if (sm > 48 * 1024)
       BDGD_CK(cudaFuncSetAttribute(k_row_fused1d<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 grid(1, ncol * p.nh);
+    bdgd_count_launch();
     k_row_fused1d<T, CPLX><<<grid, kThreads, sm, c->stream>>>(g, p, fd, x, ldx, y, ldy);
     BDGD_CK(cudaGetLastError());
     return BDGD_OK;
@@ -943,6 +956,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       size_t sm = sizeof(C) * 2 * rpb * Nx;
       if (sm > 48 * 1024)
         BDGD_CK(cudaFuncSetAttribute(k_row_fwd<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_row_fwd<T, CPLX><<<dim3(nrb, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, xc, ldx, spec, rpb);
       BDGD_CK(cudaGetLastError());
     }
@@ -956,6 +970,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       size_t sm = sizeof(C) * 2 * tx * (n + 1);
       if (sm > 48 * 1024)
         BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, mode, tx);
       BDGD_CK(cudaGetLastError());
     }
@@ -968,6 +983,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       size_t sm = sizeof(C) * 2 * tx * (n + 1);
       if (sm > 48 * 1024)
         BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, 1, tx);
       BDGD_CK(cudaGetLastError());
     }
@@ -977,6 +993,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       size_t sm = sizeof(C) * 2 * maxnf * rpb * Nx;
       if (sm > 48 * 1024)
         BDGD_CK(cudaFuncSetAttribute(k_row_inv<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
       k_row_inv<T, CPLX><<<dim3(nrb, nc * p.nh), kThreads, sm, c->stream>>>(g, p, fd, spec, xc, ldx, yc, ldy, rpb);
       BDGD_CK(cudaGetLastError());
     }
@@ -1040,9 +1057,9 @@ extern "C" int bdgd_apply(bdgd_ctx *c, int op, int prec, const void *d_x, uint64
     dim3 grid((unsigned)blocks, (unsigned)ncol);
     const unsigned char *xb = (const unsigned char *)d_x;
     unsigned char *yb = (unsigned char *)d_y;
-    if (wsz == 16) k_swap<uint4><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
-    else if (wsz == 8) k_swap<unsigned long long><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
-    else k_swap<unsigned int><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb);
+    if (wsz == 16) { bdgd_count_launch(); k_swap<uint4><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb); }
+    else if (wsz == 8) { bdgd_count_launch(); k_swap<unsigned long long><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb); }
+    else { bdgd_count_launch(); k_swap<unsigned int><<<grid, 256, 0, c->stream>>>(xb, ldxb, yb, ldyb, halfb); }
     BDGD_CK(cudaGetLastError());
     return BDGD_OK;
   }
@@ -1123,4 +1140,12 @@ extern "C" int bdgd_fft_host(bdgd_ctx *c, int forward, const void *in, void *out
   }
   BDGD_CK(cudaStreamSynchronize(c->stream));
   return BDGD_OK;
+}
+
+// Internal programs of the ground-state producer (bdg_gs.cu): 101
+// imaginary-time kinetic propagator exp(-kin_dt k^2), 102 dipolar mean field
+// of the input field.  FP64, device pointers.
+int bdgd_run_internal(bdgd_ctx *c, int kind, const void *d_x, long long ldx, void *d_y, long long ldy, int ncol) {
+  Prog p = make_prog(kind, 0);
+  return dispatch(c, p, BDGD_F64, d_x, ldx, d_y, ldy, ncol, 0, 0);
 }

@@ -526,7 +526,7 @@ static double anorm_estimate(const matmul_ctx_t *ctx) {
 static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, double *back, double *tres,
                    int want_true) {
   const int m = (int)w->m, nev = (int)w->nev, K = w->K;
-  double h[4 * 1024];
+  double *h = (double *)xcalloc(4 * (size_t)K, sizeof(double));
   DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, (uint64_t)m, B(NB_X), B(NB_AX), w->n, NULL, w->n, w->lam_d,
                         w->work, w->norms, w->norms + K, NULL));
   if (want_true) {
@@ -535,7 +535,13 @@ static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, doub
     DEV_TRY(bdgd_true_residual(dev, w->prec, w->cplx, w->S, (uint64_t)nev, w->TR, w->S, B(NB_X), w->n, w->lam_d,
                                w->work, w->norms + 2 * K, w->norms + 3 * K));
   }
-  TRY(host_vec(w, dev, w->norms, 4 * K, h));
+  {
+    int rc = host_vec(w, dev, w->norms, 4 * K, h);
+    if (rc) {
+      free(h);
+      return rc;
+    }
+  }
   for (int j = 0; j < m; j++) {
     const double rr = sqrt(h[j]), xx = sqrt(h[K + j]);
     back[j] = rr / ((anorm + fabs(lam[j])) * (xx > 0 ? xx : 1e-300));
@@ -545,6 +551,7 @@ static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, doub
       const double tt = sqrt(h[2 * K + j]), vv = sqrt(h[3 * K + j]);
       tres[j] = tt / (vv > 0 ? vv : 1e-300);
     }
+  free(h);
   return 0;
 }
 

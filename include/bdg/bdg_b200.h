@@ -67,6 +67,18 @@ void bdg_set_local_interactions_grid(bdg_t *bdg, const double *uK, const double 
 /* Full solver block after a solve: n x sizeSub column-major (host), or NULL. */
 const void *bdg_solver_block(const bdg_t *bdg);
 
+/* Stationary real condensate on the GPU: split-step imaginary-time
+ * propagation from psi_inout (dt, until |delta mu| per step < tol or
+ * max_steps), then newton_steps bordered Newton steps (CG on the BdG
+ * operator M) to the exact discrete stationary state.  H = -1/2 lap + V +
+ * g |psi|^2 (+ g_ddi Phi_dd with the reference's truncated dipolar kernel,
+ * 3D), psi normalised to sum |psi|^2 dV = 1.  Writes psi, mu, the ITP step
+ * count and ||H psi - mu psi|| (L2 with dV).  0 or a negative error. */
+int bdg_ground_state(uint64_t dim, const uint64_t *N, const double *L, const double *V, double g, double g_ddi,
+                     const double *dipole_dir, double cutoff_radius, double dt, double tol, uint64_t max_steps,
+                     int newton_steps, double *psi_inout, double *mu_out, uint64_t *steps_out,
+                     double *stationarity_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,9 @@ enum {
 
 /* Message of the last failing call of this thread. */
 const char *bdgd_last_error(void);
+/* Kernels this library has launched since load (all contexts). */
+unsigned long long bdgd_launch_count(void);
+
 /* Number of visible CUDA devices (0 without a GPU); never fails. */
 int bdgd_device_count(void);
 
@@ -118,6 +121,14 @@ typedef struct {
 
 int bdgd_gram_tasks(bdgd_ctx *ctx, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                     double *d_out);
+
+/* Ground-state producer on the context's grid (real path): split-step
+ * imaginary-time propagation then bordered Newton polish; V on the host.
+ * The dipolar kernel, when wanted, is uploaded first with
+ * bdgd_set_dipolar(enabled = 1).  See bdg_ground_state in bdg/bdg_b200.h. */
+int bdgd_ground_state(bdgd_ctx *ctx, const double *V_host, double g, double dt, double tol, int max_steps,
+                      int newton_steps, double *psi_inout, double *mu_out, int *steps_out,
+                      double *stationarity_out);
 
 #ifdef __cplusplus
 }
