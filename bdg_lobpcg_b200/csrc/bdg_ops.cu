@@ -670,6 +670,244 @@ __global__ void __launch_bounds__(256) k_row_fused1d(GeoDev g, Prog p, FieldsDev
   }
 }
 
+// ---------------------------------------------------------------------------
+// compile-time sized passes (line lengths 16..256 with radices 8/4/2/3)
+// ---------------------------------------------------------------------------
+// s-th radix of the compile-time plan: 8s first, then 4, 2, 3
+__host__ __device__ constexpr int ct_factor(int n, int s) {
+  int idx = 0;
+  while (n > 1) {
+    const int r = (n % 8 == 0) ? 8 : (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : n;
+    if (idx == s) return r;
+    n /= r;
+    ++idx;
+  }
+  return 1;
+}
+__host__ __device__ constexpr int ct_nst(int n) {
+  int c = 0;
+  while (n > 1) {
+    const int r = (n % 8 == 0) ? 8 : (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : n;
+    n /= r;
+    ++c;
+  }
+  return c;
+}
+__host__ __device__ constexpr int ct_ns(int n, int s) {
+  int p = 1;
+  for (int i = 0; i < s; ++i) p *= ct_factor(n, i);
+  return p;
+}
+// threads per line: butterflies of the first (largest-radix) stage
+__host__ __device__ constexpr int ct_tpl(int n) { return n / ct_factor(n, 0); }
+
+static bool ct_supported(int n) {
+  return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
+
+template <typename C, int N, int S, int TPL>
+__device__ __forceinline__ void ct_stage(const C *__restrict__ a, C *__restrict__ b, int lt, const C *roots,
+                                         int sgn, bool on) {
+  if (!on) return;
+  constexpr int R = ct_factor(N, S);
+  constexpr int Ns = ct_ns(N, S);
+  constexpr int nb = N / R;
+  constexpr int tw = N / (Ns * R);
+  constexpr int iters = (nb + TPL - 1) / TPL;
+#pragma unroll
+  for (int it = 0; it < iters; ++it) {
+    const int j = lt + it * TPL;
+    if ((nb % TPL == 0) || j < nb) {
+      const int k = j % Ns;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = a[j + r * nb];
+      if (Ns > 1 && k) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], rootv(roots, r * k * tw, sgn));
+      }
+      Bfly<R, C>::run(v, sgn);
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) b[base + r * Ns] = v[r];
+    }
+  }
+}
+
+// All threads of the block call this (it synchronises after every stage).
+// a/b: this thread's line in the two buffers; returns whether the result
+// ended in b (odd number of stages).
+template <typename C, int N, int TPL, int S = 0>
+__device__ __forceinline__ void ct_fft(C *a, C *b, int lt, const C *roots, int sgn, bool on) {
+  if constexpr (S < ct_nst(N)) {
+    ct_stage<C, N, S, TPL>(a, b, lt, roots, sgn, on);
+    __syncthreads();
+    ct_fft<C, N, TPL, S + 1>(b, a, lt, roots, sgn, on);
+  }
+}
+template <int N> __host__ __device__ constexpr bool ct_result_in_b() { return (ct_nst(N) % 2) == 1; }
+
+// Rows along x, forward, all NF spectra of one half per CTA (x read once).
+// grid.x: row blocks, grid.y: columns; half h fixed per launch.
+template <typename T, bool CPLX, int NX, int NF>
+__global__ void __launch_bounds__(256) k_row_fwd_ct(GeoDev g, Prog p, FieldsDev f, const void *__restrict__ xin,
+                                                    long long ldx, typename Cx<T>::t *__restrict__ spec, int h) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  constexpr int TPL = ct_tpl(NX);
+  constexpr int LPG = (256 / NF) / TPL;  // rows per field group = rows per CTA
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *a = (C *)smraw;
+  C *b = a + NF * LPG * NX;
+  const int col = blockIdx.y;
+  const V *src = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
+  const int row0 = blockIdx.x * LPG;
+  const int nr = min(LPG, g.nrows - row0);
+  for (int q = threadIdx.x; q < nr * NX; q += blockDim.x) {
+    const long long r = (long long)row0 * NX + q;
+    const V xv = src[r];
+#pragma unroll
+    for (int fi = 0; fi < NF; ++fi) a[fi * LPG * NX + q] = prologue<T, CPLX>(f, p.pre[h][fi], xv, r);
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int grp = t / (LPG * TPL);  // field
+  const int tl = t - grp * LPG * TPL;
+  const int line = tl / TPL, lt = tl - line * TPL;
+  const bool act = grp < NF;
+  const int li = act ? (grp * LPG + line) : 0;
+  ct_fft<C, NX, TPL>(a + li * NX, b + li * NX, lt, roots_of<C>(g.ax[0]), -1, act);
+  const C *res = ct_result_in_b<NX>() ? b : a;
+  const int nxk = g.nxk;
+  for (int fi = 0; fi < NF; ++fi) {
+    C *dst = spec + ((long long)col * p.J + p.j0[h] + fi) * g.H + (long long)row0 * nxk;
+    for (int q = threadIdx.x; q < nr * nxk; q += blockDim.x) {
+      const int rr = q / nxk, kx = q - rr * nxk;
+      dst[q] = res[(fi * LPG + rr) * NX + kx];
+    }
+  }
+}
+
+// Pencils along y / z with compile-time length N (see k_col_pass).
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_col_pass_ct(GeoDev g, Prog p, FieldsDev f,
+                                                     typename Cx<T>::t *__restrict__ spec, int axis, int mode) {
+  typedef typename Cx<T>::t C;
+  constexpr int TPL = ct_tpl(N);
+  constexpr int TX = 256 / TPL;  // lines (kx values) per CTA
+  constexpr int LD = N + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *a = (C *)smraw;
+  C *b = a + TX * LD;
+  const int nxk = g.nxk;
+  const int ntx = (nxk + TX - 1) / TX;
+  const int tile = blockIdx.x % ntx;
+  const int outer = blockIdx.x / ntx;
+  const int kx0 = tile * TX;
+  const int nt = min(TX, nxk - kx0);
+  long long ls, os;
+  if (axis == 1) {
+    ls = nxk;
+    os = (long long)nxk * g.N[1];
+  } else {
+    ls = (long long)nxk * g.N[1];
+    os = nxk;
+  }
+  const int job = blockIdx.y;
+  C *base = spec + (long long)job * g.H + (long long)outer * os + kx0;
+  for (int q = threadIdx.x; q < N * TX; q += blockDim.x) {
+    const int i = q / TX, t = q - i * TX;
+    if (t < nt) a[t * LD + i] = base[(long long)i * ls + t];
+  }
+  __syncthreads();
+  const int line = threadIdx.x / TPL, lt = threadIdx.x - line * TPL;
+  const bool on = line < TX;
+  const int ln = on ? line : 0;
+  const C *roots = roots_of<C>(g.ax[axis]);
+  ct_fft<C, N, TPL>(a + ln * LD, b + ln * LD, lt, roots, mode == 1 ? +1 : -1, on);
+  C *res = ct_result_in_b<N>() ? b : a;
+  C *oth = ct_result_in_b<N>() ? a : b;
+  if (mode == 2) {
+    const int col = job / p.J;
+    const int jj = job - col * p.J;
+    const int kind = p.mul[p.jh[jj]][p.jf[jj]];
+    for (int q = threadIdx.x; q < N * nt; q += blockDim.x) {
+      const int t = q / N, i = q - t * N;
+      const int ix = kx0 + t;
+      int iy, iz;
+      if (axis == 1) {
+        iy = i;
+        iz = outer;
+      } else {
+        iy = outer;
+        iz = i;
+      }
+      const long long kidx = ((long long)iz * g.N[1] + iy) * nxk + ix;
+      const double m = kmult(g, f, kind, ix, iy, iz, kidx);
+      res[t * LD + i] = cscale(res[t * LD + i], (T)m);
+    }
+    __syncthreads();
+    ct_fft<C, N, TPL>(res + ln * LD, oth + ln * LD, lt, roots, +1, on);
+    if (ct_result_in_b<N>()) res = oth;
+  }
+  for (int q = threadIdx.x; q < N * TX; q += blockDim.x) {
+    const int i = q / TX, t = q - i * TX;
+    if (t < nt) base[(long long)i * ls + t] = res[t * LD + i];
+  }
+}
+
+// Rows along x, inverse of the NF spectra of one half + epilogue.
+// grid.x: row blocks, grid.y: columns; half h fixed per launch.
+template <typename T, bool CPLX, int NX, int NF>
+__global__ void __launch_bounds__(256) k_row_inv_ct(GeoDev g, Prog p, FieldsDev f,
+                                                    const typename Cx<T>::t *__restrict__ spec,
+                                                    const void *__restrict__ xin, long long ldx,
+                                                    void *__restrict__ yout, long long ldy, int h) {
+  typedef typename El<T, CPLX>::C C;
+  typedef typename El<T, CPLX>::V V;
+  constexpr int TPL = ct_tpl(NX);
+  constexpr int LPG = (256 / NF) / TPL;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *a = (C *)smraw;
+  C *b = a + NF * LPG * NX;
+  const int nxk = g.nxk;
+  const int col = blockIdx.y;
+  const int row0 = blockIdx.x * LPG;
+  const int nr = min(LPG, g.nrows - row0);
+#pragma unroll
+  for (int fi = 0; fi < NF; ++fi) {
+    const C *src = spec + ((long long)col * p.J + p.j0[h] + fi) * g.H + (long long)row0 * nxk;
+    for (int q = threadIdx.x; q < nr * NX; q += blockDim.x) {
+      const int rr = q / NX, kx = q - rr * NX;
+      C v;
+      if (CPLX || kx < nxk)
+        v = src[rr * nxk + kx];
+      else
+        v = cconj(src[rr * nxk + (NX - kx)]);
+      a[(fi * LPG + rr) * NX + kx] = v;
+    }
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int grp = t / (LPG * TPL);
+  const int tl = t - grp * LPG * TPL;
+  const int line = tl / TPL, lt = tl - line * TPL;
+  const bool act = grp < NF;
+  const int li = act ? (grp * LPG + line) : 0;
+  ct_fft<C, NX, TPL>(a + li * NX, b + li * NX, lt, roots_of<C>(g.ax[0]), +1, act);
+  const C *res = ct_result_in_b<NX>() ? b : a;
+  const V *xs = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
+  V *ys = (V *)yout + (long long)col * ldy + (long long)h * g.S;
+  const int post = p.post[h];
+  for (int q = threadIdx.x; q < nr * NX; q += blockDim.x) {
+    const long long r = (long long)row0 * NX + q;
+    const C o0 = res[q];
+    const C o1 = (NF > 1) ? res[LPG * NX + q] : o0;
+    const V xv = (post == POST_K || post == POST_M) ? xs[r] : V();
+    ys[r] = epilogue<T, CPLX>(f, post, NF, o0, o1, xv, r);
+  }
+}
+
 // Swap: y = [x_v; x_u] (src/matmulSwap_impl.inc:18-22), copied in words of W.
 template <typename W>
 __global__ void k_swap(const unsigned char *__restrict__ x, long long ldxb, unsigned char *__restrict__ y,
@@ -904,6 +1142,95 @@ static int rows_per_block(int Nx) {
   return r < 1 ? 1 : r;
 }
 
+
+// ---- host launchers of the compile-time kernels ----
+template <typename T, bool CPLX, int NX, int NF>
+static int launch_row_fwd_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, const void *x, long long ldx,
+                             typename Cx<T>::t *spec, int nc, int h) {
+  typedef typename Cx<T>::t C;
+  constexpr int LPG = (256 / NF) / ct_tpl(NX);
+  const size_t sm = sizeof(C) * 2 * NF * LPG * NX;
+  if (sm > 48 * 1024)
+    BDGD_CK(cudaFuncSetAttribute(k_row_fwd_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int nrb = (c->geo.nrows + LPG - 1) / LPG;
+  bdgd_count_launch();
+  k_row_fwd_ct<T, CPLX, NX, NF><<<dim3(nrb, nc), 256, sm, c->stream>>>(c->geo, p, fd, x, ldx, spec, h);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+template <typename T, bool CPLX, int NX, int NF>
+static int launch_row_inv_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, const typename Cx<T>::t *spec,
+                             const void *x, long long ldx, void *y, long long ldy, int nc, int h) {
+  typedef typename Cx<T>::t C;
+  constexpr int LPG = (256 / NF) / ct_tpl(NX);
+  const size_t sm = sizeof(C) * 2 * NF * LPG * NX;
+  if (sm > 48 * 1024)
+    BDGD_CK(cudaFuncSetAttribute(k_row_inv_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int nrb = (c->geo.nrows + LPG - 1) / LPG;
+  bdgd_count_launch();
+  k_row_inv_ct<T, CPLX, NX, NF><<<dim3(nrb, nc), 256, sm, c->stream>>>(c->geo, p, fd, spec, x, ldx, y, ldy, h);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+template <typename T, int N>
+static int launch_col_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typename Cx<T>::t *spec, int njobs,
+                         int axis, int mode) {
+  typedef typename Cx<T>::t C;
+  constexpr int TX = 256 / ct_tpl(N);
+  const size_t sm = sizeof(C) * 2 * TX * (N + 1);
+  if (sm > 48 * 1024)
+    BDGD_CK(cudaFuncSetAttribute(k_col_pass_ct<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int ntx = (c->nxk + TX - 1) / TX;
+  const int outer = (axis == 1) ? c->N[2] : c->N[1];
+  bdgd_count_launch();
+  k_col_pass_ct<T, N><<<dim3(ntx * outer, njobs), 256, sm, c->stream>>>(c->geo, p, fd, spec, axis, mode);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+#define CT_SWITCH(n, CALL) \
+  switch (n) {             \
+    case 16: CALL(16);     \
+    case 32: CALL(32);     \
+    case 48: CALL(48);     \
+    case 64: CALL(64);     \
+    case 96: CALL(96);     \
+    case 128: CALL(128);   \
+    case 256: CALL(256);   \
+    default: break;        \
+  }
+
+template <typename T, bool CPLX>
+static int rows_fwd_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, const void *x, long long ldx,
+                       typename Cx<T>::t *spec, int nc, int h) {
+#define RF(NXV) return p.nf[h] == 2 ? launch_row_fwd_ct<T, CPLX, NXV, 2>(c, p, fd, x, ldx, spec, nc, h) \
+                                    : launch_row_fwd_ct<T, CPLX, NXV, 1>(c, p, fd, x, ldx, spec, nc, h)
+  CT_SWITCH(c->N[0], RF)
+#undef RF
+  return BDGD_ERR_UNSUPPORTED;
+}
+
+template <typename T, bool CPLX>
+static int rows_inv_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, const typename Cx<T>::t *spec, const void *x,
+                       long long ldx, void *y, long long ldy, int nc, int h) {
+#define RI(NXV) return p.nf[h] == 2 ? launch_row_inv_ct<T, CPLX, NXV, 2>(c, p, fd, spec, x, ldx, y, ldy, nc, h) \
+                                    : launch_row_inv_ct<T, CPLX, NXV, 1>(c, p, fd, spec, x, ldx, y, ldy, nc, h)
+  CT_SWITCH(c->N[0], RI)
+#undef RI
+  return BDGD_ERR_UNSUPPORTED;
+}
+
+template <typename T>
+static int cols_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typename Cx<T>::t *spec, int njobs, int axis,
+                   int mode) {
+#define CC(NV) return launch_col_ct<T, NV>(c, p, fd, spec, njobs, axis, mode)
+  CT_SWITCH(c->N[axis], CC)
+#undef CC
+  return BDGD_ERR_UNSUPPORTED;
+}
+
 template <typename T, bool CPLX>
 static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx, void *y, long long ldy,
                        int ncol, int only_fwd, int only_bwd) {
@@ -947,6 +1274,30 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
   if (rc) return rc;
   C *spec = (C *)c->spec;
   const int tx = f32 ? 16 : 8;
+  const bool ct = (c->dim >= 2) && ct_supported(c->N[0]) && ct_supported(c->N[1]) &&
+                  (c->dim < 3 || ct_supported(c->N[2])) && !getenv("BDG_GENERIC_FFT");
+  if (ct) {
+    for (int c0 = 0; c0 < ncol; c0 += chunk) {
+      const int nc = (ncol - c0) < chunk ? (ncol - c0) : chunk;
+      const size_t esz = CPLX ? sizeof(C) : sizeof(T);
+      const void *xc = (const char *)x + (size_t)c0 * ldx * esz;
+      void *yc = (char *)y + (size_t)c0 * ldy * esz;
+      int rc;
+      if (!only_bwd)
+        for (int h = 0; h < p.nh; ++h)
+          if ((rc = rows_fwd_ct<T, CPLX>(c, p, fd, xc, ldx, spec, nc, h))) return rc;
+      for (int ax = 1; ax < c->dim && !only_bwd; ++ax) {
+        const int last = (ax == c->dim - 1);
+        if ((rc = cols_ct<T>(c, p, fd, spec, nc * p.J, ax, (last && !only_fwd) ? 2 : 0))) return rc;
+      }
+      if (only_fwd) break;
+      for (int ax = only_bwd ? c->dim - 1 : c->dim - 2; ax >= 1; --ax)
+        if ((rc = cols_ct<T>(c, p, fd, spec, nc * p.J, ax, 1))) return rc;
+      for (int h = 0; h < p.nh; ++h)
+        if ((rc = rows_inv_ct<T, CPLX>(c, p, fd, spec, xc, ldx, yc, ldy, nc, h))) return rc;
+    }
+    return BDGD_OK;
+  }
   for (int c0 = 0; c0 < ncol; c0 += chunk) {
     const int nc = (ncol - c0) < chunk ? (ncol - c0) : chunk;
     const size_t esz = CPLX ? sizeof(C) : sizeof(T);
