@@ -627,3 +627,130 @@ extern "C" int bdgd_gather_cols(bdgd_ctx *c, const double *In, int ldi, int rows
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Gram contraction without any allocation
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory at the time they need the Gram
+// blocks: code that runs under a memory pool or arena it does not own, a
+// host framework that forbids cudaMalloc/cudaFree on its hot path (they
+// synchronise the device), or a process that has handed all device memory to
+// another allocator.  For them the split partial sums live in this fixed
+// array, which every GPU that loads the library holds until exit.
+#define BDGD_NOALLOC_SCRATCH_DOUBLES (1u << 20) /* 8 MiB */
+static __device__ __align__(256) double g_gram_noalloc_scratch[BDGD_NOALLOC_SCRATCH_DOUBLES];
+
+#define BDGD_NOALLOC_MAX_DEVICES 64
+static double *g_noalloc_ptr[BDGD_NOALLOC_MAX_DEVICES];
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side symbol is not a device address).
+static int noalloc_scratch(double **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return bdgd_check(e, "cudaGetDevice");
+  if (dev < 0 || dev >= BDGD_NOALLOC_MAX_DEVICES) {
+    bdgd_set_error("bdgd_gram_noalloc: device ordinal %d above %d", dev, BDGD_NOALLOC_MAX_DEVICES);
+    return BDGD_ERR_UNSUPPORTED;
+  }
+  if (!g_noalloc_ptr[dev]) {
+    double *p = nullptr;
+    e = cudaGetSymbolAddress((void **)&p, g_gram_noalloc_scratch);
+    if (e != cudaSuccess) return bdgd_check(e, "cudaGetSymbolAddress(g_gram_noalloc_scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_gram_noalloc(void *stream, int prec, int cplx, uint64_t half, uint64_t k, const void *d_S,
+                                 uint64_t lds, const void *d_AS, uint64_t ldas, double *d_out) {
+  if (k == 0) return BDGD_OK;
+  if (!d_S || !d_AS || !d_out) {
+    bdgd_set_error("bdgd_gram_noalloc: null pointer");
+    return BDGD_ERR_ARG;
+  }
+  const int es = cplx ? 2 : 1;
+  const unsigned long long per_split = 4ull * k * k * (unsigned long long)es;
+  if (per_split > BDGD_NOALLOC_SCRATCH_DOUBLES) {
+    bdgd_set_error("bdgd_gram_noalloc: k = %llu needs %llu bytes of scratch, above the %u-byte static buffer",
+                   (unsigned long long)k, per_split * 8ull, BDGD_NOALLOC_SCRATCH_DOUBLES * 8u);
+    return BDGD_ERR_ARG;
+  }
+  double *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  const size_t esz = (size_t)(prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
+  const char *S = (const char *)d_S, *AS = (const char *)d_AS;
+  // tasks: Guu = Su^H Su, Gvv = Sv^H Sv, Guv = Su^H Sv, Ga = S^H AS
+  GArgs g;
+  memset(&g, 0, sizeof g);
+  g.nt = 4;
+  const void *as[4] = {S, S + half * esz, S, S};
+  const void *bs[4] = {S, S + half * esz, S + half * esz, AS};
+  long long maxrows = 0;
+  int tiles = 0;
+  for (int i = 0; i < 4; ++i) {
+    GTask &t = g.t[i];
+    t.a = as[i];
+    t.b = bs[i];
+    t.lda = (long long)lds;
+    t.ldb = (long long)(i == 3 ? ldas : lds);
+    t.rows = (long long)(i == 3 ? 2 * half : half);
+    t.ka = t.kb = (int)k;
+    t.out = i;
+    t.sym = (i < 2);
+    t.ta = t.tb = (int)((k + GT - 1) / GT);
+    t.tile0 = tiles;
+    tiles += t.sym ? t.ta * (t.ta + 1) / 2 : t.ta * t.tb;
+    if (t.rows > maxrows) maxrows = t.rows;
+  }
+  g.ntiles = tiles;
+  int nsplit = (4 * 148 + tiles - 1) / tiles;
+  const int fit = (int)(BDGD_NOALLOC_SCRATCH_DOUBLES / per_split);
+  if (nsplit > fit) nsplit = fit;
+  const long long maxsplit = (maxrows + 8 * GRK - 1) / (8 * GRK);
+  if (nsplit > maxsplit) nsplit = (int)maxsplit;
+  if (nsplit < 1) nsplit = 1;
+  long long chunk = (maxrows + nsplit - 1) / nsplit;
+  chunk = (chunk + GRK - 1) / GRK * GRK;
+  if (chunk < GRK) chunk = GRK;
+  nsplit = (int)((maxrows + chunk - 1) / chunk);
+  if (nsplit < 1) nsplit = 1;
+  g.nsplit = nsplit;
+  g.chunk = chunk;
+  long long off = 0;
+  for (int i = 0; i < 4; ++i) {
+    g.t[i].part0 = off;
+    off += (long long)nsplit * g.t[i].ka * g.t[i].kb * es;
+  }
+  g.part = scratch;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t sm = sizeof(double) * GT * GLD * (cplx ? 4 : 2);
+  dim3 grid(tiles, nsplit);
+  if (prec == BDGD_F32) {
+    if (cplx) {
+      BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
+      k_gram_tasks<float, true><<<grid, 128, sm, st>>>(g);
+    } else {
+      bdgd_count_launch();
+      k_gram_tasks<float, false><<<grid, 128, sm, st>>>(g);
+    }
+  } else {
+    if (cplx) {
+      BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      bdgd_count_launch();
+      k_gram_tasks<double, true><<<grid, 128, sm, st>>>(g);
+    } else {
+      bdgd_count_launch();
+      k_gram_tasks<double, false><<<grid, 128, sm, st>>>(g);
+    }
+  }
+  BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
+  k_gram_tasks_reduce<<<dim3(32, 4), 256, 0, st>>>(g, cplx, (int)k, d_out);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+

@@ -122,6 +122,29 @@ typedef struct {
 int bdgd_gram_tasks(bdgd_ctx *ctx, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                     double *d_out);
 
+/* Gram contraction that allocates nothing (no counterpart in the reference).
+ *
+ * Same inputs and output as bdgd_gram (Guu, Gvv, Guv, Ga of a block S and
+ * its image AS, four k x k FP64 matrices, column-major, consecutive), for
+ * callers that may not allocate device memory when they need it: code
+ * running inside a memory pool or arena it does not own, or a framework
+ * that bans cudaMalloc/cudaFree on its hot path because they synchronise the
+ * device.  Nothing is allocated: no context is needed (work goes to `stream`,
+ * NULL for the default stream), and the split partial sums live in one
+ * static 8 MiB device array that each GPU using the library keeps until the
+ * process exits.
+ *
+ * Limits: the partials of one split need 4 k^2 doubles (8 k^2 complex), so k
+ * is at most 512 (real) or 362 (complex); larger k returns BDGD_ERR_ARG with
+ * a message and launches nothing.  The first call on each device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  Every call reuses the same array: calls that may run at the same
+ * time on the GPU (other streams, other host threads) race on it and must
+ * be serialised by the caller.  Each call writes every partial it reads, so
+ * nothing left over from an earlier call is used. */
+int bdgd_gram_noalloc(void *stream, int prec, int cplx, uint64_t half, uint64_t k, const void *d_S, uint64_t lds,
+                      const void *d_AS, uint64_t ldas, double *d_out);
+
 /* Ground-state producer on the context's grid (real path): split-step
  * imaginary-time propagation then bordered Newton polish; V on the host.
  * The dipolar kernel, when wanted, is uploaded first with
