@@ -165,6 +165,177 @@ __global__ void __launch_bounds__(128) k_gram_tasks(GArgs g) {
       }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined Gram kernel: tiles staged with 16-byte cp.async, two stages in
+// flight, so the loads of rows r0+RK.. overlap the DMMA work on rows r0..
+// Needs 16-byte aligned column starts (checked on the host; the kernel above
+// is the fallback).
+// ---------------------------------------------------------------------------
+template <typename T, bool CPLX> struct GStage;
+template <> struct GStage<double, false> { typedef double E; static constexpr int RK = 32, LDE = 36; };
+template <> struct GStage<float, false> { typedef float E; static constexpr int RK = 32, LDE = 36; };
+template <> struct GStage<double, true> { typedef double2 E; static constexpr int RK = 16, LDE = 18; };
+template <> struct GStage<float, true> { typedef float2 E; static constexpr int RK = 16, LDE = 18; };
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <typename E> __device__ __forceinline__ double re_of(E v);
+template <> __device__ __forceinline__ double re_of<double>(double v) { return v; }
+template <> __device__ __forceinline__ double re_of<float>(float v) { return (double)v; }
+template <> __device__ __forceinline__ double re_of<double2>(double2 v) { return v.x; }
+template <> __device__ __forceinline__ double re_of<float2>(float2 v) { return (double)v.x; }
+template <typename E> __device__ __forceinline__ double im_of(E v) { return 0.0; }
+template <> __device__ __forceinline__ double im_of<double2>(double2 v) { return v.y; }
+template <> __device__ __forceinline__ double im_of<float2>(float2 v) { return (double)v.y; }
+
+template <typename T, bool CPLX>
+__device__ __forceinline__ void stage_async(typename GStage<T, CPLX>::E *sm, const T *__restrict__ base, long long ld,
+                                            int c0, int kc, long long r0, long long rend) {
+  typedef typename GStage<T, CPLX>::E E;
+  constexpr int RK = GStage<T, CPLX>::RK, LDE = GStage<T, CPLX>::LDE;
+  constexpr int EB = (int)sizeof(E);
+  constexpr int RPC = 16 / EB;          // rows per 16-byte chunk
+  constexpr int CPC = RK / RPC;         // chunks per column
+  constexpr int ES = CPLX ? 2 : 1;
+  for (int q = threadIdx.x; q < GT * CPC; q += blockDim.x) {
+    const int c = q / CPC, ch = q - c * CPC;
+    const int r = ch * RPC;
+    const long long rr = r0 + r;
+    long long nvalid = rend - rr;
+    nvalid = nvalid < 0 ? 0 : (nvalid > RPC ? RPC : nvalid);
+    const bool colok = (c0 + c) < kc;
+    const T *src = colok && nvalid > 0 ? base + ((long long)(c0 + c) * ld + rr) * ES : base;
+    cp_async16(sm + c * LDE + r, src, colok ? (int)(nvalid * EB) : 0);
+  }
+}
+
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) k_gram_tasks2(GArgs g) {
+  typedef typename GStage<T, CPLX>::E E;
+  constexpr int RK = GStage<T, CPLX>::RK, LDE = GStage<T, CPLX>::LDE;
+  constexpr int ES = CPLX ? 2 : 1;
+  extern __shared__ __align__(16) unsigned char gsm2[];
+  E *buf = (E *)gsm2;  // [stage][A|B][GT][LDE]
+  int t = 0;
+  while (t + 1 < g.nt && (int)blockIdx.x >= g.t[t + 1].tile0) ++t;
+  const GTask tk = g.t[t];
+  int local = blockIdx.x - tk.tile0, ti, tj;
+  if (tk.sym) {
+    ti = 0;
+    int rowlen = tk.tb;
+    while (local >= rowlen) {
+      local -= rowlen;
+      ++ti;
+      rowlen = tk.tb - ti;
+    }
+    tj = ti + local;
+  } else {
+    ti = local / tk.tb;
+    tj = local - ti * tk.tb;
+  }
+  const int split = blockIdx.y;
+  const long long rbeg = (long long)split * g.chunk;
+  long long rend = rbeg + g.chunk;
+  if (rend > tk.rows) rend = tk.rows;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = warp & 1, wj = warp >> 1;
+  const int lr = lane & 3, lc = lane >> 2;
+  double acc[4][4][2], aci[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b][0] = acc[a][b][1] = 0.0;
+      aci[a][b][0] = aci[a][b][1] = 0.0;
+    }
+  const T *A = (const T *)tk.a;
+  const T *B = (const T *)tk.b;
+  const long long nst = rend > rbeg ? (rend - rbeg + RK - 1) / RK : 0;
+  if (nst > 0) {
+    stage_async<T, CPLX>(buf, A, tk.lda, ti * GT, tk.ka, rbeg, rend);
+    stage_async<T, CPLX>(buf + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg, rend);
+    cp_async_commit();
+  }
+  for (long long s = 0; s < nst; ++s) {
+    E *cur = buf + (s & 1) * 2 * GT * LDE;
+    if (s + 1 < nst) {
+      E *nxt = buf + ((s + 1) & 1) * 2 * GT * LDE;
+      const long long r0 = rbeg + (s + 1) * RK;
+      stage_async<T, CPLX>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
+      stage_async<T, CPLX>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const E *sA = cur, *sB = cur + GT * LDE;
+#pragma unroll
+    for (int kk = 0; kk < RK; kk += 4) {
+      double ar[4], br[4], ai[4], bi[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        const E v = sA[(wi * 32 + mi * 8 + lc) * LDE + kk + lr];
+        ar[mi] = re_of<E>(v);
+        ai[mi] = im_of<E>(v);
+      }
+#pragma unroll
+      for (int nj = 0; nj < 4; ++nj) {
+        const E v = sB[(wj * 32 + nj * 8 + lc) * LDE + kk + lr];
+        br[nj] = re_of<E>(v);
+        bi[nj] = im_of<E>(v);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+      if (CPLX) {
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj) {
+            dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], ar[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], -ai[mi], br[nj]);
+          }
+      }
+    }
+    __syncthreads();
+  }
+  double *out = g.part + tk.part0 + (long long)split * tk.ka * tk.kb * ES;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int i = ti * GT + wi * 32 + mi * 8 + lc;
+        const int j = tj * GT + wj * 32 + nj * 8 + 2 * lr + e;
+        if (i < tk.ka && j < tk.kb) {
+          const long long o = ((long long)j * tk.ka + i) * ES;
+          out[o] = acc[mi][nj][e];
+          if (CPLX) out[o + 1] = aci[mi][nj][e];
+        }
+      }
+}
+
+template <typename T, bool CPLX>
+static int launch_gram2(bdgd_ctx *c, const GArgs &g, dim3 grid) {
+  typedef typename GStage<T, CPLX>::E E;
+  const size_t sm = sizeof(E) * 2 * 2 * GT * GStage<T, CPLX>::LDE;
+  if (sm > 48 * 1024)
+    BDGD_CK(cudaFuncSetAttribute(k_gram_tasks2<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  bdgd_count_launch();
+  k_gram_tasks2<T, CPLX><<<grid, 128, sm, c->stream>>>(g);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
 // Sum the split partials of every task into its output block (and its
 // mirror); sym tasks read the lower triangle from the computed upper tiles.
 __global__ void k_gram_tasks_reduce(GArgs g, int cplx, int ldo, double *__restrict__ outbuf) {
@@ -257,7 +428,18 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
   // tasks with fewer rows than nsplit*chunk simply see empty splits (zeros)
   const size_t sm = sizeof(double) * GT * GLD * (cplx ? 4 : 2);
   dim3 grid(tiles, nsplit);
-  if (prec == BDGD_F32) {
+  bool aligned = !getenv("BDG_GRAM_SIMPLE");
+  {
+    const size_t eb = (size_t)(prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
+    for (int i = 0; i < ntask && aligned; ++i)
+      if (((uintptr_t)g.t[i].a | (uintptr_t)g.t[i].b) % 16 || (g.t[i].lda * eb) % 16 || (g.t[i].ldb * eb) % 16)
+        aligned = false;
+  }
+  if (aligned) {
+    if (prec == BDGD_F32) rc = cplx ? launch_gram2<float, true>(c, g, grid) : launch_gram2<float, false>(c, g, grid);
+    else rc = cplx ? launch_gram2<double, true>(c, g, grid) : launch_gram2<double, false>(c, g, grid);
+    if (rc) return rc;
+  } else if (prec == BDGD_F32) {
     if (cplx) {
       BDGD_CK(cudaFuncSetAttribute(k_gram_tasks<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       bdgd_count_launch();
@@ -754,3 +936,29 @@ extern "C" int bdgd_gram_noalloc(void *stream, int prec, int cplx, uint64_t half
   return BDGD_OK;
 }
 
+// X-X blocks of the Rayleigh-Ritz Grams for a Ritz block X (B-orthonormal,
+// A-diagonal): Ga(0:m, 0:m) = diag(lam), Guv(0:m, 0:m) = I/2 (so that
+// Guv + Guv^H = X^H B X = I).  Leading dimension ldo.
+__global__ void k_set_ritz_block(double *__restrict__ Ga, double *__restrict__ Guv, int ldo, int m, int cplx,
+                                 const double *__restrict__ lam) {
+  const int es = cplx ? 2 : 1;
+  const long long mm = (long long)m * m;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < mm; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % m), j = (int)(q / m);
+    const long long o = ((long long)j * ldo + i) * es;
+    Ga[o] = (i == j) ? lam[i] : 0.0;
+    Guv[o] = (i == j) ? 0.5 : 0.0;
+    if (cplx) {
+      Ga[o + 1] = 0.0;
+      Guv[o + 1] = 0.0;
+    }
+  }
+}
+
+extern "C" int bdgd_set_ritz_block(bdgd_ctx *c, double *Ga, double *Guv, int ldo, int m, int cplx,
+                                   const double *d_lam) {
+  bdgd_count_launch();
+  k_set_ritz_block<<<grid_for((long long)m * m), 256, 0, c->stream>>>(Ga, Guv, ldo, m, cplx, d_lam);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}

@@ -23,6 +23,7 @@ int bdgd_true_residual(bdgd_ctx *c, int prec, int cplx, uint64_t half, uint64_t 
 int bdgd_convert(bdgd_ctx *c, int to_f32, const void *src, void *dst, uint64_t n_scalars);
 int bdgd_rr_prepare(bdgd_ctx *c, const double *G, const double *Ga_in, const double *Guv, int k, int ldo, int cplx,
                     double *Gs, double *Gb, double *Ga, double *d);
+int bdgd_set_ritz_block(bdgd_ctx *c, double *Ga, double *Guv, int ldo, int m, int cplx, const double *d_lam);
 int bdgd_vec_pow(bdgd_ctx *c, const double *in, int n, double e, double *out);
 int bdgd_gather_cols(bdgd_ctx *c, const double *In, int ldi, int rows, const int *d_cols, int ncols, int cplx,
                      double *Out, int ldo);

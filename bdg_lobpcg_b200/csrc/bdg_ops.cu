@@ -705,69 +705,85 @@ static bool ct_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
 
+// Shared-memory index of line element i: one pad slot every 8 elements
+// breaks the stride-R bank conflicts of the Stockham writes.
+__host__ __device__ constexpr int ct_pad(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int ct_line(int n) { return ct_pad(n - 1) + 1; }
+
+// One in-place Stockham stage: every thread first reads all the inputs of
+// its butterflies into registers, the block synchronises, then it writes.
 template <typename C, int N, int S, int TPL>
-__device__ __forceinline__ void ct_stage(const C *__restrict__ a, C *__restrict__ b, int lt, const C *roots,
-                                         int sgn, bool on) {
-  if (!on) return;
+__device__ __forceinline__ void ct_stage(C *__restrict__ a, int lt, const C *roots, int sgn, bool on) {
   constexpr int R = ct_factor(N, S);
   constexpr int Ns = ct_ns(N, S);
   constexpr int nb = N / R;
   constexpr int tw = N / (Ns * R);
   constexpr int iters = (nb + TPL - 1) / TPL;
+  C v[iters][R];
+  if (on) {
 #pragma unroll
-  for (int it = 0; it < iters; ++it) {
-    const int j = lt + it * TPL;
-    if ((nb % TPL == 0) || j < nb) {
-      const int k = j % Ns;
-      C v[R];
+    for (int it = 0; it < iters; ++it) {
+      const int j = lt + it * TPL;
+      if ((nb % TPL == 0) || j < nb) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = a[j + r * nb];
-      if (Ns > 1 && k) {
-#pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], rootv(roots, r * k * tw, sgn));
+        for (int r = 0; r < R; ++r) v[it][r] = a[ct_pad(j + r * nb)];
       }
-      Bfly<R, C>::run(v, sgn);
-      const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-      for (int r = 0; r < R; ++r) b[base + r * Ns] = v[r];
     }
+  }
+  __syncthreads();
+  if (on) {
+#pragma unroll
+    for (int it = 0; it < iters; ++it) {
+      const int j = lt + it * TPL;
+      if ((nb % TPL == 0) || j < nb) {
+        const int k = j % Ns;
+        if (Ns > 1 && k) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) v[it][r] = cmul(v[it][r], rootv(roots, r * k * tw, sgn));
+        }
+        Bfly<R, C>::run(v[it], sgn);
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[ct_pad(base + r * Ns)] = v[it][r];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// All threads of the block call this; the result is in place in `a`
+// (this thread's line, padded layout).
+template <typename C, int N, int TPL, int S = 0>
+__device__ __forceinline__ void ct_fft(C *a, int lt, const C *roots, int sgn, bool on) {
+  if constexpr (S < ct_nst(N)) {
+    ct_stage<C, N, S, TPL>(a, lt, roots, sgn, on);
+    ct_fft<C, N, TPL, S + 1>(a, lt, roots, sgn, on);
   }
 }
 
-// All threads of the block call this (it synchronises after every stage).
-// a/b: this thread's line in the two buffers; returns whether the result
-// ended in b (odd number of stages).
-template <typename C, int N, int TPL, int S = 0>
-__device__ __forceinline__ void ct_fft(C *a, C *b, int lt, const C *roots, int sgn, bool on) {
-  if constexpr (S < ct_nst(N)) {
-    ct_stage<C, N, S, TPL>(a, b, lt, roots, sgn, on);
-    __syncthreads();
-    ct_fft<C, N, TPL, S + 1>(b, a, lt, roots, sgn, on);
-  }
-}
-template <int N> __host__ __device__ constexpr bool ct_result_in_b() { return (ct_nst(N) % 2) == 1; }
 
 // Rows along x, forward, all NF spectra of one half per CTA (x read once).
 // grid.x: row blocks, grid.y: columns; half h fixed per launch.
 template <typename T, bool CPLX, int NX, int NF>
-__global__ void __launch_bounds__(256) k_row_fwd_ct(GeoDev g, Prog p, FieldsDev f, const void *__restrict__ xin,
-                                                    long long ldx, typename Cx<T>::t *__restrict__ spec, int h) {
+__global__ void __launch_bounds__(256, 4) k_row_fwd_ct(GeoDev g, Prog p, FieldsDev f, const void *__restrict__ xin,
+                                                       long long ldx, typename Cx<T>::t *__restrict__ spec, int h) {
   typedef typename El<T, CPLX>::C C;
   typedef typename El<T, CPLX>::V V;
   constexpr int TPL = ct_tpl(NX);
-  constexpr int LPG = (256 / NF) / TPL;  // rows per field group = rows per CTA
+  constexpr int LPG = (256 / NF) / TPL;  // rows per CTA
+  constexpr int LN = ct_line(NX);        // padded line length
   extern __shared__ __align__(16) unsigned char smraw[];
-  C *a = (C *)smraw;
-  C *b = a + NF * LPG * NX;
+  C *a = (C *)smraw;                     // [NF][LPG][LN]
   const int col = blockIdx.y;
   const V *src = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
   const int row0 = blockIdx.x * LPG;
   const int nr = min(LPG, g.nrows - row0);
   for (int q = threadIdx.x; q < nr * NX; q += blockDim.x) {
+    const int rr = q / NX, ix = q - rr * NX;
     const long long r = (long long)row0 * NX + q;
     const V xv = src[r];
 #pragma unroll
-    for (int fi = 0; fi < NF; ++fi) a[fi * LPG * NX + q] = prologue<T, CPLX>(f, p.pre[h][fi], xv, r);
+    for (int fi = 0; fi < NF; ++fi) a[(fi * LPG + rr) * LN + ct_pad(ix)] = prologue<T, CPLX>(f, p.pre[h][fi], xv, r);
   }
   __syncthreads();
   const int t = threadIdx.x;
@@ -776,29 +792,28 @@ __global__ void __launch_bounds__(256) k_row_fwd_ct(GeoDev g, Prog p, FieldsDev 
   const int line = tl / TPL, lt = tl - line * TPL;
   const bool act = grp < NF;
   const int li = act ? (grp * LPG + line) : 0;
-  ct_fft<C, NX, TPL>(a + li * NX, b + li * NX, lt, roots_of<C>(g.ax[0]), -1, act);
-  const C *res = ct_result_in_b<NX>() ? b : a;
+  ct_fft<C, NX, TPL>(a + li * LN, lt, roots_of<C>(g.ax[0]), -1, act);
   const int nxk = g.nxk;
+#pragma unroll
   for (int fi = 0; fi < NF; ++fi) {
     C *dst = spec + ((long long)col * p.J + p.j0[h] + fi) * g.H + (long long)row0 * nxk;
     for (int q = threadIdx.x; q < nr * nxk; q += blockDim.x) {
       const int rr = q / nxk, kx = q - rr * nxk;
-      dst[q] = res[(fi * LPG + rr) * NX + kx];
+      dst[q] = a[(fi * LPG + rr) * LN + ct_pad(kx)];
     }
   }
 }
 
 // Pencils along y / z with compile-time length N (see k_col_pass).
 template <typename T, int N>
-__global__ void __launch_bounds__(256) k_col_pass_ct(GeoDev g, Prog p, FieldsDev f,
-                                                     typename Cx<T>::t *__restrict__ spec, int axis, int mode) {
+__global__ void __launch_bounds__(256, 4) k_col_pass_ct(GeoDev g, Prog p, FieldsDev f,
+                                                        typename Cx<T>::t *__restrict__ spec, int axis, int mode) {
   typedef typename Cx<T>::t C;
   constexpr int TPL = ct_tpl(N);
-  constexpr int TX = 256 / TPL;  // lines (kx values) per CTA
-  constexpr int LD = N + 1;
+  constexpr int TX = 256 / TPL;         // lines (kx values) per CTA
+  constexpr int LD = ct_line(N) | 1;    // odd line stride for the transposed loads
   extern __shared__ __align__(16) unsigned char smraw[];
-  C *a = (C *)smraw;
-  C *b = a + TX * LD;
+  C *a = (C *)smraw;                    // [TX][LD]
   const int nxk = g.nxk;
   const int ntx = (nxk + TX - 1) / TX;
   const int tile = blockIdx.x % ntx;
@@ -817,16 +832,14 @@ __global__ void __launch_bounds__(256) k_col_pass_ct(GeoDev g, Prog p, FieldsDev
   C *base = spec + (long long)job * g.H + (long long)outer * os + kx0;
   for (int q = threadIdx.x; q < N * TX; q += blockDim.x) {
     const int i = q / TX, t = q - i * TX;
-    if (t < nt) a[t * LD + i] = base[(long long)i * ls + t];
+    if (t < nt) a[t * LD + ct_pad(i)] = base[(long long)i * ls + t];
   }
   __syncthreads();
   const int line = threadIdx.x / TPL, lt = threadIdx.x - line * TPL;
   const bool on = line < TX;
   const int ln = on ? line : 0;
   const C *roots = roots_of<C>(g.ax[axis]);
-  ct_fft<C, N, TPL>(a + ln * LD, b + ln * LD, lt, roots, mode == 1 ? +1 : -1, on);
-  C *res = ct_result_in_b<N>() ? b : a;
-  C *oth = ct_result_in_b<N>() ? a : b;
+  ct_fft<C, N, TPL>(a + ln * LD, lt, roots, mode == 1 ? +1 : -1, on);
   if (mode == 2) {
     const int col = job / p.J;
     const int jj = job - col * p.J;
@@ -844,32 +857,32 @@ __global__ void __launch_bounds__(256) k_col_pass_ct(GeoDev g, Prog p, FieldsDev
       }
       const long long kidx = ((long long)iz * g.N[1] + iy) * nxk + ix;
       const double m = kmult(g, f, kind, ix, iy, iz, kidx);
-      res[t * LD + i] = cscale(res[t * LD + i], (T)m);
+      C &e = a[t * LD + ct_pad(i)];
+      e = cscale(e, (T)m);
     }
     __syncthreads();
-    ct_fft<C, N, TPL>(res + ln * LD, oth + ln * LD, lt, roots, +1, on);
-    if (ct_result_in_b<N>()) res = oth;
+    ct_fft<C, N, TPL>(a + ln * LD, lt, roots, +1, on);
   }
   for (int q = threadIdx.x; q < N * TX; q += blockDim.x) {
     const int i = q / TX, t = q - i * TX;
-    if (t < nt) base[(long long)i * ls + t] = res[t * LD + i];
+    if (t < nt) base[(long long)i * ls + t] = a[t * LD + ct_pad(i)];
   }
 }
 
 // Rows along x, inverse of the NF spectra of one half + epilogue.
 // grid.x: row blocks, grid.y: columns; half h fixed per launch.
 template <typename T, bool CPLX, int NX, int NF>
-__global__ void __launch_bounds__(256) k_row_inv_ct(GeoDev g, Prog p, FieldsDev f,
-                                                    const typename Cx<T>::t *__restrict__ spec,
-                                                    const void *__restrict__ xin, long long ldx,
-                                                    void *__restrict__ yout, long long ldy, int h) {
+__global__ void __launch_bounds__(256, 4) k_row_inv_ct(GeoDev g, Prog p, FieldsDev f,
+                                                       const typename Cx<T>::t *__restrict__ spec,
+                                                       const void *__restrict__ xin, long long ldx,
+                                                       void *__restrict__ yout, long long ldy, int h) {
   typedef typename El<T, CPLX>::C C;
   typedef typename El<T, CPLX>::V V;
   constexpr int TPL = ct_tpl(NX);
   constexpr int LPG = (256 / NF) / TPL;
+  constexpr int LN = ct_line(NX);
   extern __shared__ __align__(16) unsigned char smraw[];
-  C *a = (C *)smraw;
-  C *b = a + NF * LPG * NX;
+  C *a = (C *)smraw;  // [NF][LPG][LN]
   const int nxk = g.nxk;
   const int col = blockIdx.y;
   const int row0 = blockIdx.x * LPG;
@@ -884,7 +897,7 @@ __global__ void __launch_bounds__(256) k_row_inv_ct(GeoDev g, Prog p, FieldsDev 
         v = src[rr * nxk + kx];
       else
         v = cconj(src[rr * nxk + (NX - kx)]);
-      a[(fi * LPG + rr) * NX + kx] = v;
+      a[(fi * LPG + rr) * LN + ct_pad(kx)] = v;
     }
   }
   __syncthreads();
@@ -894,15 +907,15 @@ __global__ void __launch_bounds__(256) k_row_inv_ct(GeoDev g, Prog p, FieldsDev 
   const int line = tl / TPL, lt = tl - line * TPL;
   const bool act = grp < NF;
   const int li = act ? (grp * LPG + line) : 0;
-  ct_fft<C, NX, TPL>(a + li * NX, b + li * NX, lt, roots_of<C>(g.ax[0]), +1, act);
-  const C *res = ct_result_in_b<NX>() ? b : a;
+  ct_fft<C, NX, TPL>(a + li * LN, lt, roots_of<C>(g.ax[0]), +1, act);
   const V *xs = (const V *)xin + (long long)col * ldx + (long long)h * g.S;
   V *ys = (V *)yout + (long long)col * ldy + (long long)h * g.S;
   const int post = p.post[h];
   for (int q = threadIdx.x; q < nr * NX; q += blockDim.x) {
+    const int rr = q / NX, ix = q - rr * NX;
     const long long r = (long long)row0 * NX + q;
-    const C o0 = res[q];
-    const C o1 = (NF > 1) ? res[LPG * NX + q] : o0;
+    const C o0 = a[rr * LN + ct_pad(ix)];
+    const C o1 = (NF > 1) ? a[(LPG + rr) * LN + ct_pad(ix)] : o0;
     const V xv = (post == POST_K || post == POST_M) ? xs[r] : V();
     ys[r] = epilogue<T, CPLX>(f, post, NF, o0, o1, xv, r);
   }
@@ -1149,7 +1162,7 @@ static int launch_row_fwd_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, co
                              typename Cx<T>::t *spec, int nc, int h) {
   typedef typename Cx<T>::t C;
   constexpr int LPG = (256 / NF) / ct_tpl(NX);
-  const size_t sm = sizeof(C) * 2 * NF * LPG * NX;
+  const size_t sm = sizeof(C) * NF * LPG * ct_line(NX);
   if (sm > 48 * 1024)
     BDGD_CK(cudaFuncSetAttribute(k_row_fwd_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int nrb = (c->geo.nrows + LPG - 1) / LPG;
@@ -1164,7 +1177,7 @@ static int launch_row_inv_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, co
                              const void *x, long long ldx, void *y, long long ldy, int nc, int h) {
   typedef typename Cx<T>::t C;
   constexpr int LPG = (256 / NF) / ct_tpl(NX);
-  const size_t sm = sizeof(C) * 2 * NF * LPG * NX;
+  const size_t sm = sizeof(C) * NF * LPG * ct_line(NX);
   if (sm > 48 * 1024)
     BDGD_CK(cudaFuncSetAttribute(k_row_inv_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int nrb = (c->geo.nrows + LPG - 1) / LPG;
@@ -1179,7 +1192,7 @@ static int launch_col_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typena
                          int axis, int mode) {
   typedef typename Cx<T>::t C;
   constexpr int TX = 256 / ct_tpl(N);
-  const size_t sm = sizeof(C) * 2 * TX * (N + 1);
+  const size_t sm = sizeof(C) * TX * (ct_line(N) | 1);
   if (sm > 48 * 1024)
     BDGD_CK(cudaFuncSetAttribute(k_col_pass_ct<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int ntx = (c->nxk + TX - 1) / TX;

@@ -47,6 +47,7 @@
 #define DROP_F32 1e-7
 #define CLAMP_A 1e-14
 #define GUARD_LOCK 1e-12
+#define TRUE_RES_GATE 1e-7 /* backward error below which the true residual is evaluated */
 #define MIXED_SWITCH 2e-6 /* backward error at which FP32 blocks hand over to FP64 */
 
 enum { NB_X, NB_AX, NB_XN, NB_AXN, NB_P, NB_AP, NB_PN, NB_APN, NB_W, NB_AW, NB_R, NB_WT, NB_T1, NB_T2, NB_COUNT };
@@ -338,8 +339,12 @@ static bdgd_gram_task mk_task(ws_t *w, const void *a, const void *b, uint64_t ro
 }
 
 /* Rayleigh-Ritz Grams of S = [blocks] (with A-images): out0 = S^H S, out1 =
- * S^H A S, out2 = S_u^H S_v, all K x K leading dim K at w->gout. */
-static int rr_grams(ws_t *w, bdgd_ctx *dev, int nb, void *const *Sb, void *const *ASb, const int *kb) {
+ * S^H A S, out2 = S_u^H S_v, all K x K leading dim K at w->gout.
+ * With `known` (blocks [X, P, W] after the projections): the S^H S blocks of
+ * [X, P] are already in out0 (from the projection Grams), and the X-X blocks
+ * are exact for the Ritz block X: X^H A X = diag(lam), X^H B X = I (so
+ * X_u^H X_v is set to I/2); only the other blocks are contracted. */
+static int rr_grams(ws_t *w, bdgd_ctx *dev, int nb, void *const *Sb, void *const *ASb, const int *kb, int known) {
   bdgd_gram_task t[48];
   int nt = 0, off[4];
   off[0] = 0;
@@ -348,15 +353,21 @@ static int rr_grams(ws_t *w, bdgd_ctx *dev, int nb, void *const *Sb, void *const
   for (int i = 0; i < nb; i++)
     for (int j = i; j < nb; j++) {
       if (!kb[i] || !kb[j]) continue;
-      t[nt++] = mk_task(w, Sb[i], Sb[j], w->n, kb[i], kb[j], 0, off[i], off[j], i == j, i != j);
-      t[nt++] = mk_task(w, Sb[i], ASb[j], w->n, kb[i], kb[j], 1, off[i], off[j], i == j, i != j);
+      if (!(known && j < 2)) t[nt++] = mk_task(w, Sb[i], Sb[j], w->n, kb[i], kb[j], 0, off[i], off[j], i == j, i != j);
+      if (!(known && i == 0 && j == 0))
+        t[nt++] = mk_task(w, Sb[i], ASb[j], w->n, kb[i], kb[j], 1, off[i], off[j], i == j, i != j);
     }
   for (int i = 0; i < nb; i++)
     for (int j = 0; j < nb; j++) {
       if (!kb[i] || !kb[j]) continue;
+      if (known && i == 0 && j == 0) continue;
       t[nt++] = mk_task(w, Sb[i], (const char *)Sb[j] + hb, w->S, kb[i], kb[j], 2, off[i], off[j], 0, 0);
     }
   DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, nt, t, w->K, w->gout));
+  if (known) {
+    const size_t es = w->cplx ? 2 : 1, KK = (size_t)w->K * w->K * es;
+    DEV_TRY(bdgd_set_ritz_block(dev, w->gout + KK, w->gout + 2 * KK, w->K, kb[0], w->cplx, w->lam_d));
+  }
   return 0;
 }
 
@@ -529,6 +540,21 @@ static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, doub
   double *h = (double *)xcalloc(4 * (size_t)K, sizeof(double));
   DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, (uint64_t)m, B(NB_X), B(NB_AX), w->n, NULL, w->n, w->lam_d,
                         w->work, w->norms, w->norms + K, NULL));
+  if (want_true == 1) {
+    /* the true residual costs a K apply per column: evaluate it only once a
+     * wanted pair's backward error is small enough that it can be near tol */
+    int rc = host_vec(w, dev, w->norms, 2 * K, h);
+    if (rc) {
+      free(h);
+      return rc;
+    }
+    double best = INFINITY;
+    for (int j = 0; j < nev; j++) {
+      const double rr = sqrt(h[j]), xx = sqrt(h[K + j]);
+      best = fmin(best, rr / ((anorm + fabs(lam[j])) * (xx > 0 ? xx : 1e-300)));
+    }
+    if (best > TRUE_RES_GATE) want_true = 0;
+  }
   if (want_true) {
     const char *Mv = (const char *)B(NB_AX) + w->S * w->esz;
     DEV_TRY(bdgd_apply(dev, BDGD_OP_K, w->prec, Mv, w->n, w->TR, w->S, (uint64_t)nev));
@@ -546,11 +572,10 @@ static int measure(ws_t *w, bdgd_ctx *dev, double anorm, const double *lam, doub
     const double rr = sqrt(h[j]), xx = sqrt(h[K + j]);
     back[j] = rr / ((anorm + fabs(lam[j])) * (xx > 0 ? xx : 1e-300));
   }
-  if (want_true)
-    for (int j = 0; j < nev; j++) {
-      const double tt = sqrt(h[2 * K + j]), vv = sqrt(h[3 * K + j]);
-      tres[j] = tt / (vv > 0 ? vv : 1e-300);
-    }
+  for (int j = 0; j < nev; j++) {
+    const double tt = sqrt(h[2 * K + j]), vv = sqrt(h[3 * K + j]);
+    tres[j] = want_true ? tt / (vv > 0 ? vv : 1e-300) : INFINITY;
+  }
   free(h);
   return 0;
 }
@@ -568,7 +593,7 @@ typedef struct {
 /* X in B(NB_X) (m columns); runs RR on span X first.  On return lam holds the
  * m Ritz values and res_nev the convergence measure of the nev wanted pairs. */
 static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, double *lam, double *res_nev,
-                    uint64_t *iters, int *nconv_out) {
+                    uint64_t *iters, int *nconv_out, int resume) {
   cudaStream_t st = stream_of(dev);
   const int m = (int)w->m, nev = (int)w->nev, K = w->K;
   const size_t es = w->cplx ? 2 : 1;
@@ -586,7 +611,7 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   {
     void *Sb[1] = {B(NB_X)}, *ASb[1] = {B(NB_AX)};
     int kb[1] = {m};
-    TRY(rr_grams(w, dev, 1, Sb, ASb, kb));
+    TRY(rr_grams(w, dev, 1, Sb, ASb, kb, 0));
   }
   TRY(rayleigh_ritz(w, dev, m, m, drop, lam, &nsel));
   if (nsel < m) {
@@ -598,11 +623,18 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   swapb(w, NB_X, NB_XN);
   swapb(w, NB_AX, NB_AXN);
   CUDA_TRY(cudaMemcpyAsync(w->lam_d, lam, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (resume && w->p > 0) {
+    /* continue with the search direction P handed over by the previous phase */
+    TRY(deflate_block(w, dev, B(NB_P), w->p));
+    DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, B(NB_P), w->n, B(NB_AP), w->n, (uint64_t)w->p));
+    ss->cols_apply_A += (uint64_t)w->p;
+  } else {
+    w->p = 0;
+  }
   cudaEventRecord(w->ev[2], st);
   CUDA_TRY(cudaEventSynchronize(w->ev[2]));
-  ss->ms_apply_A += ev_ms(w->ev[0], w->ev[1]);
+  ss->ms_apply_A += ev_ms(w->ev[0], w->ev[2]);
   ss->cols_apply_A += (uint64_t)m;
-  w->p = 0;
   uint64_t it = 0;
   int nconv = 0;
   const int want_true = (o->criterion == BDG_CONV_TRUE_RESIDUAL);
@@ -642,9 +674,9 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
       TRY(gram_pinv_apply(w, dev, w->gout, m, K, w->gout + (size_t)m * K * es, p, drop, w->Cs));
       TRY(bgemm(w, dev, B(NB_X), m, w->Cs, m, p, -1.0, 1.0, B(NB_P)));
       TRY(bgemm(w, dev, B(NB_AX), m, w->Cs, m, p, -1.0, 1.0, B(NB_AP)));
-      t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 0, 0, 0, 1, 0);
+      t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 1, 0, 0, 1, 0);
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
-      TRY(svqb(w, dev, w->gout, p, K, drop, w->Cs, &pk));
+      TRY(svqb(w, dev, w->gout + (size_t)K * K * es, p, K, drop, w->Cs, &pk));
       /* Cs holds Z_P (p x pk, leading dim p) */
       TRY(bgemm(w, dev, B(NB_P), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T1)));
       TRY(bgemm(w, dev, B(NB_AP), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T2)));
@@ -656,7 +688,7 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     {
       bdgd_gram_task t[5];
       int nt = 0;
-      t[nt++] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0);
+      if (p == 0) t[nt++] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0); /* else kept from above */
       t[nt++] = mk_task(w, B(NB_X), B(NB_WT), w->n, m, na, 0, 0, q, 0, 0);
       if (pk > 0) {
         t[nt++] = mk_task(w, B(NB_X), B(NB_P), w->n, m, pk, 0, 0, m, 0, 1);
@@ -668,11 +700,11 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
       /* Cs: q x na (leading dim q) */
       TRY(bgemm(w, dev, B(NB_X), m, w->Cs, q, na, -1.0, 1.0, B(NB_WT)));
       if (pk > 0) TRY(bgemm(w, dev, B(NB_P), pk, w->Cs + (size_t)m * es, q, na, -1.0, 1.0, B(NB_WT)));
-      t[0] = mk_task(w, B(NB_WT), B(NB_WT), w->n, na, na, 0, 0, 0, 1, 0);
+      t[0] = mk_task(w, B(NB_WT), B(NB_WT), w->n, na, na, 1, 0, 0, 1, 0);
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
     }
     int wk = 0;
-    TRY(svqb(w, dev, w->gout, na, K, drop, w->Cs, &wk));
+    TRY(svqb(w, dev, w->gout + (size_t)K * K * es, na, K, drop, w->Cs, &wk));
     TRY(bgemm(w, dev, B(NB_WT), na, w->Cs, na, wk, 1.0, 0.0, B(NB_W)));
     cudaEventRecord(w->ev[6], st);
     DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, B(NB_W), w->n, B(NB_AW), w->n, (uint64_t)wk));
@@ -682,7 +714,7 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     {
       void *Sb[3] = {B(NB_X), B(NB_P), B(NB_W)}, *ASb[3] = {B(NB_AX), B(NB_AP), B(NB_AW)};
       int kb[3] = {m, pk, wk};
-      TRY(rr_grams(w, dev, 3, Sb, ASb, kb));
+      TRY(rr_grams(w, dev, 3, Sb, ASb, kb, 1));
     }
     cudaEventRecord(w->ev[8], st);
     TRY(rayleigh_ritz(w, dev, k, m, drop, lam, &nsel));
@@ -742,9 +774,12 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   return 0;
 }
 
-/* copy the FP32 block X (and nothing else) into a fresh FP64 workspace */
+/* hand the FP32 phase's X and P blocks to the FP64 workspace */
 static int to_f64(ws_t *w32, ws_t *w64, bdgd_ctx *dev) {
-  DEV_TRY(bdgd_convert(dev, 0, w32->blk[NB_X], w64->blk[NB_X], w32->n * w32->m * (w32->cplx ? 2 : 1)));
+  const uint64_t es = w32->cplx ? 2 : 1;
+  DEV_TRY(bdgd_convert(dev, 0, w32->blk[NB_X], w64->blk[NB_X], w32->n * w32->m * es));
+  w64->p = w32->p;
+  if (w32->p > 0) DEV_TRY(bdgd_convert(dev, 0, w32->blk[NB_P], w64->blk[NB_P], w32->n * (uint64_t)w32->p * es));
   return 0;
 }
 
@@ -810,10 +845,12 @@ static int solve_gpu(bdg_t *bdg) {
   if (mixed) {
     loop_opts_t o32 = o;
     o32.criterion = BDG_CONV_BACKWARD;
-    o32.tol = fmax(bdg->tol, MIXED_SWITCH);
+    const char *sw = getenv("BDG_MIXED_SWITCH");
+    const double sw_at = sw ? atof(sw) : MIXED_SWITCH;
+    o32.tol = fmax(bdg->tol, sw_at);
     o32.stop_backward_at_floor = 1;
-    o32.floor = MIXED_SWITCH;
-    rc = run_loop(w, dev, bdg, &o32, lam, res, &iters, &nconv);
+    o32.floor = sw_at;
+    rc = run_loop(w, dev, bdg, &o32, lam, res, &iters, &nconv, 0);
     if (!rc) {
       ws_t *w64 = &wsp[0];
       if ((rc = ws_setup(w64, dev, S, m, nev, cplx, BDGD_F64))) return rc;
@@ -822,11 +859,11 @@ static int solve_gpu(bdg_t *bdg) {
       if ((rc = to_f64(w, w64, dev))) return rc;
       w = w64;
       o.maxit = bdg->maxIter > iters ? bdg->maxIter - iters : 0;
-      rc = run_loop(w, dev, bdg, &o, lam, res, &iters2, &nconv);
+      rc = run_loop(w, dev, bdg, &o, lam, res, &iters2, &nconv, 1);
       bdg->stats.refine_iterations = iters2;
     }
   } else {
-    rc = run_loop(w, dev, bdg, &o, lam, res, &iters, &nconv);
+    rc = run_loop(w, dev, bdg, &o, lam, res, &iters, &nconv, 0);
   }
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);
@@ -843,7 +880,7 @@ static int solve_gpu(bdg_t *bdg) {
   /* final measures of the wanted pairs */
   {
     double back[1024], tres[1024];
-    TRY(measure(w, dev, anorm, lam, back, tres, 1));
+    TRY(measure(w, dev, anorm, lam, back, tres, 2));
     double mx = 0.0, mt = 0.0;
     for (uint64_t j = 0; j < nev; j++) {
       mx = fmax(mx, res[j]);
