@@ -37,6 +37,7 @@ struct FieldsDev {
   double mu;
   double inv_size;
   double kin_dt;  // exp(-kin_dt k^2) multiplier of the imaginary-time step
+  const double *ptab;  // preconditioner multiplier per spectrum point (H), or null
 };
 
 struct bdgd_ctx {
@@ -70,6 +71,7 @@ struct bdgd_ctx {
   size_t gram_part_bytes;
   size_t spec_cap;  // max scratch bytes per apply chunk
   double kin_dt;
+  double *ptab;     // (1/size) / safe_val(mu + k^2/2) per spectrum point, for the current mu
 };
 
 int bdgd_run_internal(bdgd_ctx *c, int kind, const void *d_x, long long ldx, void *d_y, long long ldy, int ncol);

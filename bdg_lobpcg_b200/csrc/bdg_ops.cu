@@ -28,6 +28,8 @@
 #include <string.h>
 
 #include "bdg_dev.h"
+#include "bdg_kern.cuh"
+#include "bdg_lines.h"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -72,145 +74,6 @@ int bdgd_ensure(void **ptr, size_t *have, size_t want) {
   return BDGD_OK;
 }
 
-// ---------------------------------------------------------------------------
-// complex helpers
-// ---------------------------------------------------------------------------
-template <typename T> struct Cx;
-template <> struct Cx<double> { typedef double2 t; };
-template <> struct Cx<float> { typedef float2 t; };
-
-template <typename C> __device__ __forceinline__ C cmk(double a, double b) {
-  C r;
-  r.x = a;
-  r.y = b;
-  return r;
-}
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
-  C r;
-  r.x = a.x + b.x;
-  r.y = a.y + b.y;
-  return r;
-}
-template <typename C> __device__ __forceinline__ C csub(C a, C b) {
-  C r;
-  r.x = a.x - b.x;
-  r.y = a.y - b.y;
-  return r;
-}
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
-  C r;
-  r.x = a.x * b.x - a.y * b.y;
-  r.y = a.x * b.y + a.y * b.x;
-  return r;
-}
-template <typename C> __device__ __forceinline__ C cconj(C a) {
-  a.y = -a.y;
-  return a;
-}
-template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) {
-  a.x *= s;
-  a.y *= s;
-  return a;
-}
-// (x + i y) * (sgn * i)
-template <typename C> __device__ __forceinline__ C cmul_si(C a, int sgn) {
-  C r;
-  if (sgn > 0) {
-    r.x = -a.y;
-    r.y = a.x;
-  } else {
-    r.x = a.y;
-    r.y = -a.x;
-  }
-  return r;
-}
-
-template <typename C> __device__ __forceinline__ const C *roots_of(const AxisDev &ax);
-template <> __device__ __forceinline__ const double2 *roots_of<double2>(const AxisDev &ax) {
-  return ax.r64;
-}
-template <> __device__ __forceinline__ const float2 *roots_of<float2>(const AxisDev &ax) {
-  return ax.r32;
-}
-
-// root(m) = exp(sgn * 2 pi i m / n)
-template <typename C> __device__ __forceinline__ C rootv(const C *r, int m, int sgn) {
-  C w = __ldg(r + m);
-  if (sgn > 0) w.y = -w.y;
-  return w;
-}
-
-// ---------------------------------------------------------------------------
-// small DFT butterflies (in registers)
-// ---------------------------------------------------------------------------
-template <typename C> __device__ __forceinline__ void bfly2(C *v) {
-  C a = v[0];
-  v[0] = cadd(a, v[1]);
-  v[1] = csub(a, v[1]);
-}
-
-template <typename C> __device__ __forceinline__ void bfly4(C &v0, C &v1, C &v2, C &v3, int sgn) {
-  C a0 = cadd(v0, v2), a1 = csub(v0, v2);
-  C a2 = cadd(v1, v3), a3 = cmul_si(csub(v1, v3), sgn);
-  v0 = cadd(a0, a2);
-  v2 = csub(a0, a2);
-  v1 = cadd(a1, a3);
-  v3 = csub(a1, a3);
-}
-
-template <typename C> __device__ __forceinline__ void bfly8(C *v, int sgn) {
-  // even/odd split: E = DFT4(v0 v2 v4 v6), O = DFT4(v1 v3 v5 v7)
-  bfly4(v[0], v[2], v[4], v[6], sgn);
-  bfly4(v[1], v[3], v[5], v[7], sgn);
-  const double h = 0.70710678118654752440;
-  C o1 = v[3], o2 = v[5], o3 = v[7];
-  // o1 * exp(sgn i pi/4) = h (x - sgn y) + i h (sgn x + y)
-  C t1, t3;
-  t1.x = h * (o1.x - sgn * o1.y);
-  t1.y = h * (sgn * o1.x + o1.y);
-  C t2 = cmul_si(o2, sgn);
-  // o3 * exp(sgn i 3pi/4) = h(-x - sgn y) + i h(sgn x - y)
-  t3.x = h * (-o3.x - sgn * o3.y);
-  t3.y = h * (sgn * o3.x - o3.y);
-  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  C o0 = v[1];
-  v[0] = cadd(e0, o0);
-  v[4] = csub(e0, o0);
-  v[1] = cadd(e1, t1);
-  v[5] = csub(e1, t1);
-  v[2] = cadd(e2, t2);
-  v[6] = csub(e2, t2);
-  v[3] = cadd(e3, t3);
-  v[7] = csub(e3, t3);
-}
-
-template <typename C> __device__ __forceinline__ void bfly3(C *v, int sgn) {
-  const double h = 0.86602540378443864676;
-  C t1 = cadd(v[1], v[2]);
-  C t2;
-  t2.x = v[0].x - 0.5 * t1.x;
-  t2.y = v[0].y - 0.5 * t1.y;
-  C t3 = cscale(cmul_si(csub(v[1], v[2]), sgn), h);
-  v[0] = cadd(v[0], t1);
-  v[1] = cadd(t2, t3);
-  v[2] = csub(t2, t3);
-}
-
-template <int R, typename C> struct Bfly {
-  static __device__ __forceinline__ void run(C *v, int sgn) {}
-};
-template <typename C> struct Bfly<2, C> {
-  static __device__ __forceinline__ void run(C *v, int) { bfly2(v); }
-};
-template <typename C> struct Bfly<3, C> {
-  static __device__ __forceinline__ void run(C *v, int sgn) { bfly3(v, sgn); }
-};
-template <typename C> struct Bfly<4, C> {
-  static __device__ __forceinline__ void run(C *v, int sgn) { bfly4(v[0], v[1], v[2], v[3], sgn); }
-};
-template <typename C> struct Bfly<8, C> {
-  static __device__ __forceinline__ void run(C *v, int sgn) { bfly8(v, sgn); }
-};
 
 // One Stockham stage of radix R over `nlines` lines of length n in shared
 // memory (line l at a + l*ls), a -> b.
@@ -293,23 +156,6 @@ __device__ C *smem_fft(C *a, C *b, int nlines, int ls, const AxisDev &ax, int sg
   return a;
 }
 
-// ---------------------------------------------------------------------------
-// operator programs
-// ---------------------------------------------------------------------------
-enum { PRE_NONE = 0, PRE_PK, PRE_PM, PRE_CONJWF, PRE_DENS, PRE_XDENS };
-enum { MUL_KIN = 0, MUL_DIP, MUL_PRE, MUL_ONE, MUL_EXPKIN };
-enum { POST_RAW = 0, POST_K, POST_M, POST_TK, POST_TM, POST_DIPCONV, POST_PHI };
-
-struct Prog {
-  int nh;         // halves per column (1, or 2 for [u; v])
-  int J;          // spectra (jobs) per column
-  int nf[2];      // spectra per half
-  int j0[2];      // first job of each half
-  int pre[2][2];  // prologue per half, field
-  int mul[2][2];  // k-space multiplier per half, field
-  int post[2];    // epilogue per half
-  int jh[4], jf[4];
-};
 
 static Prog make_prog(int op, int dipolar) {
   Prog p;
@@ -355,78 +201,6 @@ static Prog make_prog(int op, int dipolar) {
   return p;
 }
 
-// k-space multiplier of spectrum element (ix, iy, iz), flat index kidx.
-// Same arithmetic as the reference loops: k2 = kx2[0][ix] + kx2[1][iy] +
-// kx2[2][iz]; kinetic k2 * (0.5/size) (src/kinetic_impl.inc:25-27); dipolar
-// kernel * (1/size) (src/dipolar_conv_impl.inc:41-43); preconditioner
-// (1/size) / safe_val(mu + 0.5 k2) (src/precond_impl.inc:45-48).
-__device__ __forceinline__ double kmult(const GeoDev &g, const FieldsDev &f, int kind, int ix, int iy,
-                                        int iz, long long kidx) {
-  if (kind == MUL_DIP) return __ldg(f.vdd + kidx) * f.inv_size;
-  if (kind == MUL_ONE) return 1.0;
-  double k2 = __ldg(g.kx2[0] + ix);
-  if (g.dim > 1) k2 += __ldg(g.kx2[1] + iy);
-  if (g.dim > 2) k2 += __ldg(g.kx2[2] + iz);
-  if (kind == MUL_KIN) return k2 * (0.5 * f.inv_size);
-  if (kind == MUL_EXPKIN) return exp(-f.kin_dt * k2) * f.inv_size;
-  double d = f.mu + 0.5 * k2;
-  if (fabs(d) < 1e-8) d = 1e-8;
-  return f.inv_size / d;
-}
-
-// ---------------------------------------------------------------------------
-// element access helpers for the real (T) and complex (C) paths
-// ---------------------------------------------------------------------------
-template <typename T, bool CPLX> struct El;
-template <typename T> struct El<T, false> {
-  typedef typename Cx<T>::t C;
-  typedef T V;
-  static __device__ __forceinline__ C to_c(V v) { return cmk<C>(v, 0.0); }
-  static __device__ __forceinline__ V from_c(C c) { return c.x; }
-};
-template <typename T> struct El<T, true> {
-  typedef typename Cx<T>::t C;
-  typedef C V;
-  static __device__ __forceinline__ C to_c(V v) { return v; }
-  static __device__ __forceinline__ V from_c(C c) { return c; }
-};
-
-template <typename T, bool CPLX>
-__device__ __forceinline__ typename El<T, CPLX>::C prologue(const FieldsDev &f, int kind,
-                                                            typename El<T, CPLX>::V x, long long r) {
-  typedef typename El<T, CPLX>::C C;
-  typedef typename El<T, CPLX>::V V;
-  const T *pK = (const T *)f.pK;
-  const T *pM = (const T *)f.pM;
-  const V *w = (const V *)f.w;
-  if constexpr (CPLX) {
-    switch (kind) {
-      case PRE_PK: return cscale(x, __ldg(pK + r));
-      case PRE_PM: return cscale(x, __ldg(pM + r));
-      case PRE_CONJWF: return cmul(cconj(w[r]), x);
-      case PRE_DENS: {
-        // |psi|^2 as cabs(psi)^2 (src/dipolar_meanfield_impl.inc:33-35)
-        C z = w[r];
-        T a = hypot(z.x, z.y);
-        return cmk<C>(a * a, 0.0);
-      }
-      case PRE_XDENS: return cmk<C>(x.x * x.x + x.y * x.y, 0.0);
-      default: return x;
-    }
-  } else {
-    switch (kind) {
-      case PRE_PK: return cmk<C>(__ldg(pK + r) * x, 0.0);
-      case PRE_PM: return cmk<C>(__ldg(pM + r) * x, 0.0);
-      case PRE_CONJWF: return cmk<C>(w[r] * x, 0.0);
-      case PRE_DENS: {
-        T a = fabs(w[r]);
-        return cmk<C>(a * a, 0.0);
-      }
-      case PRE_XDENS: return cmk<C>(x * x, 0.0);
-      default: return cmk<C>(x, 0.0);
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // pass kernels
@@ -526,57 +300,6 @@ __global__ void __launch_bounds__(256) k_col_pass(GeoDev g, Prog p, FieldsDev f,
   }
 }
 
-// Epilogue of one half at real-space point r given the inverse transforms
-// o0 (and o1 for M with dipolar exchange).  Reference arithmetic order:
-//   K: y = kin + ltK*x                      (src/matmulK_impl.inc:21-23)
-//   M: y = kin + (ltM*x + 2*(g*wf*buf))     (src/matmulM_impl.inc:30-32, dipolar_conv :49-51)
-//   T: y = out * p                          (src/precond_impl.inc:56-60)
-template <typename T, bool CPLX>
-__device__ __forceinline__ typename El<T, CPLX>::V epilogue(const FieldsDev &f, int post, int nf,
-                                                            typename El<T, CPLX>::C o0,
-                                                            typename El<T, CPLX>::C o1,
-                                                            typename El<T, CPLX>::V x, long long r) {
-  typedef typename El<T, CPLX>::V V;
-  typedef typename El<T, CPLX>::C C;
-  const T *ltK = (const T *)f.ltK;
-  const T *ltM = (const T *)f.ltM;
-  const T *pK = (const T *)f.pK;
-  const T *pM = (const T *)f.pM;
-  const V *w = (const V *)f.w;
-  const T g = (T)f.g_ddi;
-  if constexpr (CPLX) {
-    switch (post) {
-      case POST_K: return cadd(o0, cscale(x, __ldg(ltK + r)));
-      case POST_M:
-        if (nf > 1) {
-          C dc = cmul(cscale(w[r], g), o1);
-          return cadd(o0, cadd(cscale(x, __ldg(ltM + r)), cscale(dc, (T)2)));
-        }
-        return cadd(o0, cscale(x, __ldg(ltM + r)));
-      case POST_TK: return cscale(o0, __ldg(pK + r));
-      case POST_TM: return cscale(o0, __ldg(pM + r));
-      case POST_DIPCONV: return cmul(cscale(w[r], g), o0);
-      case POST_PHI: return cmk<C>(g * o0.x, 0.0);
-      default: return o0;
-    }
-  } else {
-    const T y0 = o0.x;
-    switch (post) {
-      case POST_K: return y0 + __ldg(ltK + r) * x;
-      case POST_M:
-        if (nf > 1) {
-          const T dc = (g * w[r]) * o1.x;
-          return y0 + (__ldg(ltM + r) * x + (T)2 * dc);
-        }
-        return y0 + __ldg(ltM + r) * x;
-      case POST_TK: return y0 * __ldg(pK + r);
-      case POST_TM: return y0 * __ldg(pM + r);
-      case POST_DIPCONV: return (g * w[r]) * o0.x;
-      case POST_PHI: return g * o0.x;
-      default: return y0;
-    }
-  }
-}
 
 // Rows along x, inverse + epilogue.  grid.x: row blocks, grid.y: ncol*nh units.
 template <typename T, bool CPLX>
@@ -1074,8 +797,8 @@ extern "C" void bdgd_destroy(bdgd_ctx **pc) {
     cudaFree(c->d_roots32[d]);
     cudaFree(c->d_kx2[d]);
   }
-  void *bufs[] = {c->ltK64, c->ltM64, c->pK64, c->pM64, c->ltK32, c->ltM32, c->pK32,
-                  c->pM32,  c->wf64,  c->wf32, c->vdd,  c->spec,  c->io,    c->gram_part};
+  void *bufs[] = {c->ltK64, c->ltM64, c->pK64, c->pM64, c->ltK32, c->ltM32, c->pK32, c->pM32,
+                  c->wf64,  c->wf32,  c->vdd,  c->spec, c->io,    c->gram_part, c->ptab};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1086,6 +809,37 @@ extern "C" void bdgd_destroy(bdgd_ctx **pc) {
 extern "C" void *bdgd_stream(bdgd_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 extern "C" int bdgd_synchronize(bdgd_ctx *c) {
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  return BDGD_OK;
+}
+
+// Preconditioner multiplier table for the current mu: the k-space factor of
+// T at every spectrum point, computed by kmult itself (bit-identical to the
+// on-the-fly value); read once per spectrum pass instead of a division per
+// element.
+__global__ void k_ptab(GeoDev g, FieldsDev f, double *__restrict__ out) {
+  const long long n = g.H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.nxk);
+    const long long r = i / g.nxk;
+    const int iy = g.dim > 1 ? (int)(r % g.N[1]) : 0;
+    const int iz = g.dim > 2 ? (int)(r / g.N[1]) : 0;
+    out[i] = kmult(g, f, MUL_PRE, ix, iy, iz, i);
+  }
+}
+
+static int build_ptab(bdgd_ctx *c) {
+  if (!c->ptab) BDGD_CK(cudaMalloc((void **)&c->ptab, sizeof(double) * c->H));
+  FieldsDev f;
+  memset(&f, 0, sizeof f);
+  f.mu = c->mu;
+  f.inv_size = 1.0 / (double)c->S;
+  f.ptab = nullptr;
+  long long blocks = (c->H + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  bdgd_count_launch();
+  k_ptab<<<(unsigned)blocks, 256, 0, c->stream>>>(c->geo, f, c->ptab);
+  BDGD_CK(cudaGetLastError());
   BDGD_CK(cudaStreamSynchronize(c->stream));
   return BDGD_OK;
 }
@@ -1118,7 +872,7 @@ extern "C" int bdgd_set_precond(bdgd_ctx *c, const double *sK, const double *sM,
   if (sM && (rc = upload_pair(c, &c->pM64, &c->pM32, sM, c->S))) return rc;
   c->mu = mu;
   c->has_precond = (sK && sM) ? 1 : c->has_precond;
-  return BDGD_OK;
+  return build_ptab(c);
 }
 
 extern "C" int bdgd_set_wavefunction(bdgd_ctx *c, const void *wf) {
@@ -1244,6 +998,21 @@ static int cols_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typename Cx<
   return BDGD_ERR_UNSUPPORTED;
 }
 
+// FFT pass family: register line transforms (default), compile-time sized
+// shared-memory stages, or the generic runtime-sized kernels.  BDG_FFT_PATH
+// = reg | ct | generic overrides (BDG_GENERIC_FFT=1 is the same as generic).
+enum { FFT_PATH_REG = 0, FFT_PATH_CT = 1, FFT_PATH_GENERIC = 2 };
+static int fft_path(const bdgd_ctx *c) {
+  (void)c;
+  if (getenv("BDG_GENERIC_FFT")) return FFT_PATH_GENERIC;
+  const char *e = getenv("BDG_FFT_PATH");
+  if (e) {
+    if (!strcmp(e, "ct")) return FFT_PATH_CT;
+    if (!strcmp(e, "generic")) return FFT_PATH_GENERIC;
+  }
+  return FFT_PATH_REG;
+}
+
 template <typename T, bool CPLX>
 static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx, void *y, long long ldy,
                        int ncol, int only_fwd, int only_bwd) {
@@ -1260,6 +1029,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
   fd.mu = c->mu;
   fd.inv_size = 1.0 / (double)c->S;
   fd.kin_dt = c->kin_dt;
+  fd.ptab = c->ptab;
   const GeoDev &g = c->geo;
   const int Nx = c->N[0];
   const int rpb = rows_per_block(Nx);
@@ -1287,8 +1057,19 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
   if (rc) return rc;
   C *spec = (C *)c->spec;
   const int tx = f32 ? 16 : 8;
+  if (!only_fwd && !only_bwd && fft_path(c) == FFT_PATH_REG && bdgd_lines_usable(c, p)) {
+    for (int c0 = 0; c0 < ncol; c0 += chunk) {
+      const int nc = (ncol - c0) < chunk ? (ncol - c0) : chunk;
+      const size_t esz = CPLX ? sizeof(C) : sizeof(T);
+      const void *xc = (const char *)x + (size_t)c0 * ldx * esz;
+      void *yc = (char *)y + (size_t)c0 * ldy * esz;
+      int rc = bdgd_lines_apply(c, p, fd, f32 ? BDGD_F32 : BDGD_F64, xc, ldx, yc, ldy, spec, nc);
+      if (rc) return rc;
+    }
+    return BDGD_OK;
+  }
   const bool ct = (c->dim >= 2) && ct_supported(c->N[0]) && ct_supported(c->N[1]) &&
-                  (c->dim < 3 || ct_supported(c->N[2])) && !getenv("BDG_GENERIC_FFT");
+                  (c->dim < 3 || ct_supported(c->N[2])) && fft_path(c) != FFT_PATH_GENERIC;
   if (ct) {
     for (int c0 = 0; c0 < ncol; c0 += chunk) {
       const int nc = (ncol - c0) < chunk ? (ncol - c0) : chunk;

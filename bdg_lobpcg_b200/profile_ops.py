@@ -1,14 +1,37 @@
-"""Run a fixed number of batched operator applies for profiling (ncu).
+"""Batched operator applies for profiling (ncu) and timing.
 
     python -m bdg_lobpcg_b200.profile_ops [--grid 128] [--ncol 8] [--prec 0|1] [--reps 3]
+                                          [--complex] [--time] [--paths reg,ct]
 
-Random fields and columns on a grid^3 dipolar context; applies LREP and TLREP
-`reps` times each (after one warm-up apply), then a Gram of the block.
+Random fields and columns on a grid^3 dipolar context.  Without --time it
+applies LREP and TLREP `reps` times each (after one warm-up apply), then one
+Gram of the block: a fixed launch sequence for ncu.  With --time it times
+`reps` applies of each operator per FFT pass family with CUDA events on the
+library's stream and prints one JSON line per (path, operator) with the
+milliseconds per apply and the bandwidth of the algorithmic bytes (the
+three-pass FFT round-trip model: per column K = 3e*S + 4*ec*H,
+M = 3e*S + 8*ec*H with the dipolar exchange, T_Lrep = 2*(2e*S + 4*ec*H),
+e the real-space and ec the spectrum element size, H the spectrum points
+per field).
 """
 import argparse
+import json
+import os
 import sys
 
 import numpy as np
+
+
+def model_bytes(op, S, H, e, ec, dipolar=True):
+    """Algorithmic bytes per column: e real-space and ec spectrum element size
+    (real FP64: 8 and 16; complex FP64: 16 and 16; FP32 halves)."""
+    k = 3 * e * S + 4 * ec * H
+    m = 3 * e * S + (8 if dipolar else 4) * ec * H
+    if op == "LREP":
+        return k + m
+    if op == "TLREP":
+        return 2 * (2 * e * S + 4 * ec * H)
+    raise ValueError(op)
 
 
 def main():
@@ -17,6 +40,9 @@ def main():
     ap.add_argument("--ncol", type=int, default=8)
     ap.add_argument("--prec", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--complex", action="store_true")
+    ap.add_argument("--time", action="store_true")
+    ap.add_argument("--paths", default="reg,ct")
     a = ap.parse_args()
     import torch
 
@@ -24,22 +50,49 @@ def main():
 
     N = [a.grid] * 3
     S = a.grid ** 3
-    H = (a.grid // 2 + 1) * a.grid * a.grid
+    H = S if a.complex else (a.grid // 2 + 1) * a.grid * a.grid
     rng = np.random.default_rng(0)
-    dc = B.DeviceContext(3, N, [24.0] * 3, False)
-    dc.set_fields(ltK=1 + rng.random(S), ltM=2 + rng.random(S), wf=rng.random(S), pK=rng.random(S) + 0.5,
+    dc = B.DeviceContext(3, N, [24.0] * 3, a.complex)
+    wf = rng.random(S) + (1j * rng.random(S) if a.complex else 0)
+    dc.set_fields(ltK=1 + rng.random(S), ltM=2 + rng.random(S), wf=wf, pK=rng.random(S) + 0.5,
                   pM=rng.random(S) + 0.5, mu=1.0, vdd=rng.standard_normal(H), g_ddi=0.5, dipolar=True)
-    dt = torch.float32 if a.prec else torch.float64
+    if a.complex:
+        dt = torch.complex64 if a.prec else torch.complex128
+    else:
+        dt = torch.float32 if a.prec else torch.float64
     x = torch.randn(a.ncol, 2 * S, dtype=dt, device="cuda")
     y = torch.empty_like(x)
     torch.cuda.synchronize()
-    for op in (B.OP_LREP, B.OP_TLREP):
-        for _ in range(1 + a.reps):
-            dc.apply_ptr(op, a.prec, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, a.ncol)
-    out = torch.zeros(4 * a.ncol * a.ncol, dtype=torch.float64, device="cuda")
-    dc.gram_ptr(a.prec, False, S, a.ncol, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, out.data_ptr())
-    dc.synchronize()
-    print("profile_ops done", a)
+    if not a.time:
+        for op in (B.OP_LREP, B.OP_TLREP):
+            for _ in range(1 + a.reps):
+                dc.apply_ptr(op, a.prec, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, a.ncol)
+        out = torch.zeros(4 * a.ncol * a.ncol * (2 if a.complex else 1), dtype=torch.float64, device="cuda")
+        dc.gram_ptr(a.prec, a.complex, S, a.ncol, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, out.data_ptr())
+        dc.synchronize()
+        print("profile_ops done", a)
+        return 0
+    stream = torch.cuda.ExternalStream(dc.stream)
+    e = (4 if a.prec else 8) * (2 if a.complex else 1)
+    ec = 2 * (4 if a.prec else 8)
+    for path in a.paths.split(","):
+        os.environ["BDG_FFT_PATH"] = path
+        for name, op in (("LREP", B.OP_LREP), ("TLREP", B.OP_TLREP)):
+            for _ in range(2):
+                dc.apply_ptr(op, a.prec, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, a.ncol)
+            dc.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(a.reps):
+                dc.apply_ptr(op, a.prec, x.data_ptr(), 2 * S, y.data_ptr(), 2 * S, a.ncol)
+            t1.record(stream)
+            t1.synchronize()
+            ms = t0.elapsed_time(t1) / a.reps
+            gb = model_bytes(name, S, H, e, ec) * a.ncol / 1e9
+            print(json.dumps({"path": path, "op": name, "grid": a.grid, "ncol": a.ncol, "prec": a.prec,
+                              "complex": a.complex, "ms_per_apply": ms, "ms_per_col": ms / a.ncol,
+                              "model_GB": gb, "model_GBps": gb / (ms / 1e3)}))
     return 0
 
 
