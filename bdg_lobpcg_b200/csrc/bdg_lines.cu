@@ -214,6 +214,101 @@ __device__ __forceinline__ C czero() {
   return z;
 }
 
+
+// ---------------------------------------------------------------------------
+// prologue / epilogue with the coefficient loads hoisted: the operator kind
+// is uniform over a launch, so the array it reads is chosen once and every
+// load of a row chunk is issued before the arithmetic (a per-element switch
+// with the load inside would expose one memory latency per element).  The
+// arithmetic is that of prologue() and epilogue() in bdg_kern.cuh.
+// ---------------------------------------------------------------------------
+// real-valued coefficient array of a prologue kind (pK, pM; the wavefunction
+// for the real path), or null
+__device__ __forceinline__ const void *pre_coef(const FieldsDev &f, int kind) {
+  switch (kind) {
+    case PRE_PK: return f.pK;
+    case PRE_PM: return f.pM;
+    case PRE_CONJWF:
+    case PRE_DENS: return f.w;
+    default: return nullptr;
+  }
+}
+template <typename T>
+__device__ __forceinline__ T pre_real(int kind, T x, T c) {
+  switch (kind) {
+    case PRE_PK:
+    case PRE_PM:
+    case PRE_CONJWF: return c * x;
+    case PRE_DENS: {
+      const T a = fabs(c);
+      return a * a;
+    }
+    case PRE_XDENS: return x * x;
+    default: return x;
+  }
+}
+// complex path: c is the real coefficient (pK, pM), w the wavefunction value
+template <typename T, typename C>
+__device__ __forceinline__ C pre_cplx(int kind, C x, T c, C w) {
+  switch (kind) {
+    case PRE_PK:
+    case PRE_PM: return cscale(x, c);
+    case PRE_CONJWF: return cmul(cconj(w), x);
+    case PRE_DENS: {
+      const T a = hypot(w.x, w.y);
+      return cmk<C>(a * a, 0.0);
+    }
+    case PRE_XDENS: return cmk<C>(x.x * x.x + x.y * x.y, 0.0);
+    default: return x;
+  }
+}
+// real-valued coefficient array of an epilogue kind (ltK, ltM, pK, pM), or null
+__device__ __forceinline__ const void *post_coef(const FieldsDev &f, int post) {
+  switch (post) {
+    case POST_K: return f.ltK;
+    case POST_M: return f.ltM;
+    case POST_TK: return f.pK;
+    case POST_TM: return f.pM;
+    default: return nullptr;
+  }
+}
+template <typename T>
+__device__ __forceinline__ T epi_real(int post, int nf, T y0, T y1, T x, T c, T w, T g) {
+  switch (post) {
+    case POST_K: return y0 + c * x;
+    case POST_M:
+      if (nf > 1) {
+        const T dc = (g * w) * y1;
+        return y0 + (c * x + (T)2 * dc);
+      }
+      return y0 + c * x;
+    case POST_TK:
+    case POST_TM: return y0 * c;
+    case POST_DIPCONV: return (g * w) * y0;
+    case POST_PHI: return g * y0;
+    default: return y0;
+  }
+}
+template <typename T, typename C>
+__device__ __forceinline__ C epi_cplx(int post, int nf, C o0, C o1, C x, T c, C w, T g) {
+  switch (post) {
+    case POST_K: return cadd(o0, cscale(x, c));
+    case POST_M:
+      if (nf > 1) {
+        const C dc = cmul(cscale(w, g), o1);
+        return cadd(o0, cadd(cscale(x, c), cscale(dc, (T)2)));
+      }
+      return cadd(o0, cscale(x, c));
+    case POST_TK:
+    case POST_TM: return cscale(o0, c);
+    case POST_DIPCONV: return cmul(cscale(w, g), o0);
+    case POST_PHI: return cmk<C>(g * o0.x, 0.0);
+    default: return o0;
+  }
+}
+// elements per load batch of the epilogue (bounds the registers in flight)
+constexpr int kEpiBatch = 8;
+
 // ---------------------------------------------------------------------------
 // pencil pass along axis 1 or 2 (MODE 0 forward, 1 inverse, 2 forward *
 // k-space multiplier * inverse).  Lines are the spectrum lines along the
@@ -334,17 +429,32 @@ __global__ void __launch_bounds__(128, 3) k_rows_fwd_reg(GeoDev g, Prog p, Field
     const long long ra = (NF == 1 ? 2 * Lc : Lc) * N;
     const long long rb = (NF == 1) ? ra + N : ra;
     const int ka = p.pre[h][0], kb = p.pre[h][NF == 1 ? 0 : 1];
+    const T *ca = (const T *)pre_coef(f, ka), *cb = (const T *)pre_coef(f, kb);
+    T xa[P::N1], xb[P::N1], wa[P::N1], wb[P::N1];
 #pragma unroll
     for (int n1 = 0; n1 < P::N1; ++n1) {
-      const int n = P::N2 * n1 + t;
-      if (on) {
-        const T xa = src[ra + n];
-        const T xb = (NF == 1) ? src[rb + n] : xa;
-        v[n1].x = prologue<T, false>(f, ka, xa, ra + n).x;
-        v[n1].y = prologue<T, false>(f, kb, xb, rb + n).x;
-      } else {
-        v[n1] = czero<C>();
+      xa[n1] = xb[n1] = wa[n1] = wb[n1] = (T)0;
+    }
+    if (on) {
+#pragma unroll
+      for (int n1 = 0; n1 < P::N1; ++n1) xa[n1] = src[ra + P::N2 * n1 + t];
+      if (NF == 1) {
+#pragma unroll
+        for (int n1 = 0; n1 < P::N1; ++n1) xb[n1] = src[rb + P::N2 * n1 + t];
       }
+      if (ca) {
+#pragma unroll
+        for (int n1 = 0; n1 < P::N1; ++n1) wa[n1] = __ldg(ca + ra + P::N2 * n1 + t);
+      }
+      if (cb) {
+#pragma unroll
+        for (int n1 = 0; n1 < P::N1; ++n1) wb[n1] = __ldg(cb + rb + P::N2 * n1 + t);
+      }
+    }
+#pragma unroll
+    for (int n1 = 0; n1 < P::N1; ++n1) {
+      v[n1].x = pre_real<T>(ka, xa[n1], wa[n1]);
+      v[n1].y = pre_real<T>(kb, (NF == 1) ? xb[n1] : xa[n1], wb[n1]);
     }
     line_dft<C, N, -1>(v, lb, t, roots);
     __syncthreads();  // phase-2 reads done before the line area is reused
@@ -380,11 +490,29 @@ __global__ void __launch_bounds__(128, 3) k_rows_fwd_reg(GeoDev g, Prog p, Field
     const int fi = (int)(Lc - row * NF);
     const int kind = p.pre[h][fi];
     const long long r0 = row * N;
+    const T *cr = (kind == PRE_PK || kind == PRE_PM) ? (const T *)pre_coef(f, kind) : nullptr;
+    const C *cw = (kind == PRE_CONJWF || kind == PRE_DENS) ? (const C *)f.w : nullptr;
+    C xv[P::N1], wv[P::N1];
+    T rv[P::N1];
 #pragma unroll
     for (int n1 = 0; n1 < P::N1; ++n1) {
-      const int n = P::N2 * n1 + t;
-      v[n1] = on ? prologue<T, true>(f, kind, src[r0 + n], r0 + n) : czero<C>();
+      xv[n1] = wv[n1] = czero<C>();
+      rv[n1] = (T)0;
     }
+    if (on) {
+#pragma unroll
+      for (int n1 = 0; n1 < P::N1; ++n1) xv[n1] = src[r0 + P::N2 * n1 + t];
+      if (cr) {
+#pragma unroll
+        for (int n1 = 0; n1 < P::N1; ++n1) rv[n1] = __ldg(cr + r0 + P::N2 * n1 + t);
+      }
+      if (cw) {
+#pragma unroll
+        for (int n1 = 0; n1 < P::N1; ++n1) wv[n1] = cw[r0 + P::N2 * n1 + t];
+      }
+    }
+#pragma unroll
+    for (int n1 = 0; n1 < P::N1; ++n1) v[n1] = on ? pre_cplx<T, C>(kind, xv[n1], rv[n1], wv[n1]) : czero<C>();
     line_dft<C, N, -1>(v, lb, t, roots);
     if (on) {
       C *s = spec + ((long long)col * p.J + p.j0[h] + fi) * g.H + row * N;
@@ -461,25 +589,36 @@ __global__ void __launch_bounds__(128, 3) k_rows_inv_reg(GeoDev g, Prog p, Field
     line_dft<C, N, +1>(v, lb, t, roots);
     if (on) {
       const long long ra = (NF == 1 ? 2 * Lc : Lc) * N;
-      const long long rb = ra + N;
+      const T *cl = (const T *)post_coef(f, post);
+      const bool needw = (post == POST_M && NF > 1) || post == POST_DIPCONV;
+      const T *wr = (const T *)f.w;
+      const T gg = (T)f.g_ddi;
+      // NF = 1: rows ra (real parts) and ra + N (imaginary parts); NF = 2: row ra
 #pragma unroll
-      for (int j = 0; j < P::Q; ++j)
+      for (int rr = 0; rr < (NF == 1 ? 2 : 1); ++rr) {
+        const long long ro = ra + rr * N;
 #pragma unroll
-        for (int k2 = 0; k2 < P::N2; ++k2) {
-          const int n = t + P::N2 * j + P::N1 * k2;
-          const C o = v[j * P::N2 + k2];
-          C oa, ob;
-          oa.x = o.x;
-          oa.y = 0;
-          ob.x = o.y;
-          ob.y = 0;
-          if (NF == 1) {
-            ys[ra + n] = epilogue<T, false>(f, post, 1, oa, oa, needx ? xs[ra + n] : (T)0, ra + n);
-            ys[rb + n] = epilogue<T, false>(f, post, 1, ob, ob, needx ? xs[rb + n] : (T)0, rb + n);
-          } else {
-            ys[ra + n] = epilogue<T, false>(f, post, 2, oa, ob, needx ? xs[ra + n] : (T)0, ra + n);
+        for (int e0 = 0; e0 < P::N1; e0 += kEpiBatch) {
+          T xv[kEpiBatch], cv[kEpiBatch], wv[kEpiBatch];
+#pragma unroll
+          for (int b = 0; b < kEpiBatch; ++b) {
+            const int e = e0 + b;
+            const int n = t + P::N2 * (e / P::N2) + P::N1 * (e % P::N2);
+            xv[b] = (needx && e < P::N1) ? xs[ro + n] : (T)0;
+            cv[b] = (cl && e < P::N1) ? __ldg(cl + ro + n) : (T)0;
+            wv[b] = (needw && e < P::N1) ? wr[ro + n] : (T)0;
+          }
+#pragma unroll
+          for (int b = 0; b < kEpiBatch; ++b) {
+            const int e = e0 + b;
+            if (e < P::N1) {
+              const int n = t + P::N2 * (e / P::N2) + P::N1 * (e % P::N2);
+              const T y0 = rr ? v[e].y : v[e].x;
+              ys[ro + n] = epi_real<T>(post, NF, y0, v[e].y, xv[b], cv[b], wv[b], gg);
+            }
           }
         }
+      }
     }
   } else {
     const long long r0 = Lc * N;
@@ -496,15 +635,33 @@ __global__ void __launch_bounds__(128, 3) k_rows_inv_reg(GeoDev g, Prog p, Field
       line_dft<C, N, +1>(w, lb, t, roots);
     }
     if (on) {
+      const T *cl = (const T *)post_coef(f, post);
+      const bool needw = (post == POST_M && NF > 1) || post == POST_DIPCONV;
+      const C *wc = (const C *)f.w;
+      const T gg = (T)f.g_ddi;
 #pragma unroll
-      for (int j = 0; j < P::Q; ++j)
+      for (int e0 = 0; e0 < P::N1; e0 += kEpiBatch) {
+        C xv[kEpiBatch], wv[kEpiBatch];
+        T cv[kEpiBatch];
 #pragma unroll
-        for (int k2 = 0; k2 < P::N2; ++k2) {
-          const int n = t + P::N2 * j + P::N1 * k2;
-          const C o0 = v[j * P::N2 + k2];
-          const C o1 = (NF > 1) ? w[(NF > 1) ? j * P::N2 + k2 : 0] : o0;
-          ys[r0 + n] = epilogue<T, true>(f, post, NF, o0, o1, needx ? xs[r0 + n] : czero<C>(), r0 + n);
+        for (int b = 0; b < kEpiBatch; ++b) {
+          const int e = e0 + b;
+          const int n = t + P::N2 * (e / P::N2) + P::N1 * (e % P::N2);
+          xv[b] = (needx && e < P::N1) ? xs[r0 + n] : czero<C>();
+          cv[b] = (cl && e < P::N1) ? __ldg(cl + r0 + n) : (T)0;
+          wv[b] = (needw && e < P::N1) ? wc[r0 + n] : czero<C>();
         }
+#pragma unroll
+        for (int b = 0; b < kEpiBatch; ++b) {
+          const int e = e0 + b;
+          if (e < P::N1) {
+            const int n = t + P::N2 * (e / P::N2) + P::N1 * (e % P::N2);
+            const C o0 = v[e];
+            const C o1 = (NF > 1) ? w[(NF > 1) ? e : 0] : o0;
+            ys[r0 + n] = epi_cplx<T, C>(post, NF, o0, o1, xv[b], cv[b], wv[b], gg);
+          }
+        }
+      }
     }
   }
 }
