@@ -35,6 +35,8 @@ struct GTask {
   int ta, tb;          // tiles along a, b
   int tile0;           // first global tile of this task
   long long part0;     // offset of this task's partials (doubles)
+  long long rowsP;     // rows rounded up to the stage height (stream-K work per tile)
+  long long wbase;     // start of this task's tiles on the stream-K work line
 };
 
 struct GArgs {
@@ -324,6 +326,272 @@ __global__ void __launch_bounds__(128) k_gram_tasks2(GArgs g) {
       }
 }
 
+// ---------------------------------------------------------------------------
+// Stream-K schedule of the pipelined Gram kernel.  The (tile, row) work of
+// all tasks is laid on one line -- task after task, tile after tile, each
+// tile's rows rounded up to a multiple of the stage height -- and cut into
+// equal pieces, one per resident block, so every block has the same work
+// whatever the mix of task sizes (tasks over the u or v half have half the
+// rows of those over all n).  A block writes one GT x GT partial per tile
+// segment it covers; a tile's partials are summed in a fixed order by the
+// reduction, so the result is deterministic.
+// ---------------------------------------------------------------------------
+#define GSK_STEP 32        // work-line granularity (multiple of every stage height)
+#define GMAXTILES 1024
+
+struct GArgsSK {
+  GTask t[GMAXT];
+  int nt;
+  int ntiles;
+  long long per;  // work-line rows per block (multiple of GSK_STEP)
+  long long W;    // work-line length
+  double *part;
+  int segbase[GMAXTILES + 1];  // first partial slot of each tile
+};
+
+__device__ __forceinline__ void gram_tile_of(const GTask &tk, int local, int &ti, int &tj) {
+  if (tk.sym) {
+    ti = 0;
+    int rowlen = tk.tb;
+    while (local >= rowlen) {
+      local -= rowlen;
+      ++ti;
+      rowlen = tk.tb - ti;
+    }
+    tj = ti + local;
+  } else {
+    ti = local / tk.tb;
+    tj = local - ti * tk.tb;
+  }
+}
+
+// One tile of A^H B over rows [rbeg, rend): the two-stage cp.async pipeline
+// of k_gram_tasks2; writes the GT x GT partial to out (column-major, tile-local).
+template <typename T, bool CPLX>
+__device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, long long rbeg, long long rend,
+                                               double *__restrict__ out, typename GStage<T, CPLX>::E *buf) {
+  typedef typename GStage<T, CPLX>::E E;
+  constexpr int RK = GStage<T, CPLX>::RK, LDE = GStage<T, CPLX>::LDE;
+  constexpr int ES = CPLX ? 2 : 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = warp & 1, wj = warp >> 1;
+  const int lr = lane & 3, lc = lane >> 2;
+  double acc[4][4][2], aci[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b][0] = acc[a][b][1] = 0.0;
+      aci[a][b][0] = aci[a][b][1] = 0.0;
+    }
+  const T *A = (const T *)tk.a;
+  const T *B = (const T *)tk.b;
+  const long long nst = rend > rbeg ? (rend - rbeg + RK - 1) / RK : 0;
+  if (nst > 0) {
+    stage_async<T, CPLX>(buf, A, tk.lda, ti * GT, tk.ka, rbeg, rend);
+    stage_async<T, CPLX>(buf + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg, rend);
+    cp_async_commit();
+  }
+  for (long long s = 0; s < nst; ++s) {
+    E *cur = buf + (s & 1) * 2 * GT * LDE;
+    if (s + 1 < nst) {
+      E *nxt = buf + ((s + 1) & 1) * 2 * GT * LDE;
+      const long long r0 = rbeg + (s + 1) * RK;
+      stage_async<T, CPLX>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
+      stage_async<T, CPLX>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const E *sA = cur, *sB = cur + GT * LDE;
+#pragma unroll
+    for (int kk = 0; kk < RK; kk += 4) {
+      double ar[4], br[4], ai[4], bi[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        const E v = sA[(wi * 32 + mi * 8 + lc) * LDE + kk + lr];
+        ar[mi] = re_of<E>(v);
+        ai[mi] = im_of<E>(v);
+      }
+#pragma unroll
+      for (int nj = 0; nj < 4; ++nj) {
+        const E v = sB[(wj * 32 + nj * 8 + lc) * LDE + kk + lr];
+        br[nj] = re_of<E>(v);
+        bi[nj] = im_of<E>(v);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+      if (CPLX) {
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj) {
+            dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], ar[mi], bi[nj]);
+            dmma(aci[mi][nj][0], aci[mi][nj][1], -ai[mi], br[nj]);
+          }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int il = wi * 32 + mi * 8 + lc;
+        const int jl = wj * 32 + nj * 8 + 2 * lr + e;
+        const long long o = ((long long)jl * GT + il) * ES;
+        out[o] = acc[mi][nj][e];
+        if (CPLX) out[o + 1] = aci[mi][nj][e];
+      }
+}
+
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) k_gram_sk(GArgsSK g) {
+  typedef typename GStage<T, CPLX>::E E;
+  constexpr int ES = CPLX ? 2 : 1;
+  extern __shared__ __align__(16) unsigned char gsm3[];
+  E *buf = (E *)gsm3;
+  const long long start = (long long)blockIdx.x * g.per;
+  long long end = start + g.per;
+  if (end > g.W) end = g.W;
+  long long pos = start;
+  int t = 0;
+  while (pos < end) {
+    while (t + 1 < g.nt && pos >= g.t[t + 1].wbase) ++t;
+    const GTask &tk = g.t[t];
+    const long long rel = pos - tk.wbase;
+    const int lt = (int)(rel / tk.rowsP);
+    const long long r0 = rel - (long long)lt * tk.rowsP;
+    long long seglen = tk.rowsP - r0;
+    if (seglen > end - pos) seglen = end - pos;
+    long long r1 = r0 + seglen;
+    if (r1 > tk.rows) r1 = tk.rows;
+    int ti, tj;
+    gram_tile_of(tk, lt, ti, tj);
+    const int tau = tk.tile0 + lt;
+    const long long first = (tk.wbase + (long long)lt * tk.rowsP) / g.per;
+    const int slot = g.segbase[tau] + (int)((long long)blockIdx.x - first);
+    gram_tile_rows<T, CPLX>(tk, ti, tj, r0, r1, g.part + (long long)slot * GT * GT * ES, buf);
+    pos += seglen;
+  }
+}
+
+// Sum the segment partials of every tile into the output block (and its
+// mirror); symmetric tasks take the lower triangle from the upper tiles.
+__global__ void k_gram_sk_reduce(GArgsSK g, int cplx, int ldo, double *__restrict__ outbuf) {
+  const int es = cplx ? 2 : 1;
+  const int t = blockIdx.y;
+  const GTask &tk = g.t[t];
+  const long long kk = (long long)tk.ka * tk.kb;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < kk; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % tk.ka), j = (int)(q / tk.ka);
+    int si = i, sj = j;
+    bool conj = false;
+    if (tk.sym && (i / GT) > (j / GT)) {
+      si = j;
+      sj = i;
+      conj = true;
+    }
+    const int ti = si / GT, tj = sj / GT;
+    const int lt = tk.sym ? (ti * tk.tb - ti * (ti - 1) / 2 + (tj - ti)) : (ti * tk.tb + tj);
+    const int tau = tk.tile0 + lt;
+    const long long el = ((long long)(sj - tj * GT) * GT + (si - ti * GT)) * es;
+    double re = 0.0, im = 0.0;
+    for (int sg = g.segbase[tau]; sg < g.segbase[tau + 1]; ++sg) {
+      const double *pp = g.part + (long long)sg * GT * GT * es + el;
+      re += pp[0];
+      if (cplx) im += pp[1];
+    }
+    if (conj) im = -im;
+    double *o = outbuf + (long long)tk.out * ldo * ldo * es;
+    const long long dst = ((long long)(tk.j0 + j) * ldo + tk.i0 + i) * es;
+    o[dst] = re;
+    if (cplx) o[dst + 1] = im;
+    if (tk.mirror) {
+      const long long mdst = ((long long)(tk.i0 + i) * ldo + tk.j0 + j) * es;
+      o[mdst] = re;
+      if (cplx) o[mdst + 1] = -im;
+    }
+  }
+}
+
+// resident blocks of k_gram_sk<T, CPLX> on this device (cached per device)
+template <typename T, bool CPLX>
+static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
+  static int cached[64];
+  const int dev = c->device < 64 ? c->device : 63;
+  if (cached[dev]) return cached[dev];
+  int nsm = 0, nb = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX>, 128, sm) != cudaSuccess || nb < 1 ||
+      nsm < 1) {
+    cudaGetLastError();
+    return 148;
+  }
+  cached[dev] = nb * nsm;
+  return cached[dev];
+}
+
+// Stream-K launch of the task list; returns BDGD_ERR_UNSUPPORTED when the
+// tile count exceeds GMAXTILES (the caller then uses the row-split kernels).
+template <typename T, bool CPLX>
+static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, double *d_out) {
+  typedef typename GStage<T, CPLX>::E E;
+  const int es = cplx ? 2 : 1;
+  if (ga.ntiles > GMAXTILES) return BDGD_ERR_UNSUPPORTED;
+  const size_t sm = sizeof(E) * 2 * 2 * GT * GStage<T, CPLX>::LDE;
+  if (sm > 48 * 1024) BDGD_CK(cudaFuncSetAttribute(k_gram_sk<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  static thread_local GArgsSK g;  // large; host-side staging of the kernel parameters
+  memset(&g, 0, sizeof g);
+  g.nt = ga.nt;
+  g.ntiles = ga.ntiles;
+  long long W = 0;
+  for (int i = 0; i < ga.nt; ++i) {
+    g.t[i] = ga.t[i];
+    GTask &t = g.t[i];
+    t.rowsP = (t.rows + GSK_STEP - 1) / GSK_STEP * GSK_STEP;
+    t.wbase = W;
+    const int nti = t.sym ? t.ta * (t.ta + 1) / 2 : t.ta * t.tb;
+    W += (long long)nti * t.rowsP;
+  }
+  if (W == 0) return BDGD_OK;
+  const int slots = gram_sk_slots<T, CPLX>(c, sm);
+  long long per = (W + slots - 1) / slots;
+  per = (per + GSK_STEP - 1) / GSK_STEP * GSK_STEP;
+  const long long nblk = (W + per - 1) / per;
+  g.per = per;
+  g.W = W;
+  int sb = 0;
+  for (int i = 0; i < g.nt; ++i) {
+    const GTask &t = g.t[i];
+    const int nti = t.sym ? t.ta * (t.ta + 1) / 2 : t.ta * t.tb;
+    for (int lt = 0; lt < nti; ++lt) {
+      const long long b0 = t.wbase + (long long)lt * t.rowsP;
+      const long long f = b0 / per, l = (b0 + t.rowsP - 1) / per;
+      g.segbase[t.tile0 + lt] = sb;
+      if (t.rowsP > 0) sb += (int)(l - f + 1);  // a task without rows has no segments (its blocks are zero)
+    }
+  }
+  g.segbase[g.ntiles] = sb;
+  int rc = bdgd_ensure((void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * (size_t)sb * GT * GT * es);
+  if (rc) return rc;
+  g.part = c->gram_part;
+  bdgd_count_launch();
+  k_gram_sk<T, CPLX><<<(unsigned)nblk, 128, sm, c->stream>>>(g);
+  BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
+  k_gram_sk_reduce<<<dim3(32, g.nt), 256, 0, c->stream>>>(g, cplx, ldo, d_out);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
 template <typename T, bool CPLX>
 static int launch_gram2(bdgd_ctx *c, const GArgs &g, dim3 grid) {
   typedef typename GStage<T, CPLX>::E E;
@@ -434,6 +702,13 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
     for (int i = 0; i < ntask && aligned; ++i)
       if (((uintptr_t)g.t[i].a | (uintptr_t)g.t[i].b) % 16 || (g.t[i].lda * eb) % 16 || (g.t[i].ldb * eb) % 16)
         aligned = false;
+  }
+  if (aligned && !getenv("BDG_GRAM_SPLIT")) {
+    if (prec == BDGD_F32) rc = cplx ? launch_gram_sk<float, true>(c, g, cplx, ldo, d_out)
+                                    : launch_gram_sk<float, false>(c, g, cplx, ldo, d_out);
+    else rc = cplx ? launch_gram_sk<double, true>(c, g, cplx, ldo, d_out)
+                   : launch_gram_sk<double, false>(c, g, cplx, ldo, d_out);
+    if (rc != BDGD_ERR_UNSUPPORTED) return rc;
   }
   if (aligned) {
     if (prec == BDGD_F32) rc = cplx ? launch_gram2<float, true>(c, g, grid) : launch_gram2<float, false>(c, g, grid);

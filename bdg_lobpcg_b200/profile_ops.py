@@ -2,6 +2,7 @@
 
     python -m bdg_lobpcg_b200.profile_ops [--grid 128] [--ncol 8] [--prec 0|1] [--reps 3]
                                           [--complex] [--time] [--paths reg,ct]
+    python -m bdg_lobpcg_b200.profile_ops --gram 192 [--grid 128] [--prec 0|1] [--reps 5]
 
 Random fields and columns on a grid^3 dipolar context.  Without --time it
 applies LREP and TLREP `reps` times each (after one warm-up apply), then one
@@ -13,6 +14,12 @@ three-pass FFT round-trip model: per column K = 3e*S + 4*ec*H,
 M = 3e*S + 8*ec*H with the dipolar exchange, T_Lrep = 2*(2e*S + 4*ec*H),
 e the real-space and ec the spectrum element size, H the spectrum points
 per field).
+
+With --gram K it times bdgd_gram (Guu, Gvv, Guv and Ga of a K-column block
+on 2*grid^3 rows) and, for reference, cuBLAS FP64 through torch on the same
+contraction (S S^T and S AS^T of the K x n blocks) and on a square 8192^3
+FP64 GEMM, and prints the FLOP rates.  The library counts a symmetric block
+at tile granularity (64 x 64 tiles on and above the diagonal).
 """
 import argparse
 import json
@@ -43,8 +50,12 @@ def main():
     ap.add_argument("--complex", action="store_true")
     ap.add_argument("--time", action="store_true")
     ap.add_argument("--paths", default="reg,ct")
+    ap.add_argument("--gram", type=int, default=0)
     a = ap.parse_args()
     import torch
+
+    if a.gram:
+        return gram_main(a)
 
     import bdg_lobpcg_b200 as B
 
@@ -93,6 +104,56 @@ def main():
             print(json.dumps({"path": path, "op": name, "grid": a.grid, "ncol": a.ncol, "prec": a.prec,
                               "complex": a.complex, "ms_per_apply": ms, "ms_per_col": ms / a.ncol,
                               "model_GB": gb, "model_GBps": gb / (ms / 1e3)}))
+    return 0
+
+
+def _time(fn, stream, reps):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(reps):
+        fn()
+    t1.record(stream)
+    t1.synchronize()
+    return t0.elapsed_time(t1) / reps
+
+
+def gram_main(a):
+    import torch
+
+    import bdg_lobpcg_b200 as B
+
+    k, S = a.gram, a.grid ** 3
+    n = 2 * S
+    dt = torch.float32 if a.prec else torch.float64
+    dc = B.DeviceContext(3, [a.grid] * 3, [24.0] * 3, False)
+    X = torch.randn(k, n, dtype=dt, device="cuda")
+    AX = torch.randn(k, n, dtype=dt, device="cuda")
+    out = torch.zeros(4 * k * k, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(dc.stream)
+
+    def lib():
+        dc.gram_ptr(a.prec, False, S, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr())
+
+    ms = _time(lib, stream, a.reps)
+    tiles = (k + 63) // 64
+    symfrac = tiles * (tiles + 1) / 2 / (tiles * tiles)
+    flops_exec = 2.0 * S * k * k * (2 * symfrac + 1) + 2.0 * n * k * k
+    flops_min = 2.0 * S * k * k * 2 + 2.0 * n * k * k  # Guu, Gvv half each + Guv + Ga
+    print(json.dumps({"what": "bdgd_gram", "k": k, "rows": n, "prec": a.prec, "ms": ms,
+                      "tflops_executed": flops_exec / ms / 1e9, "tflops_useful": flops_min / ms / 1e9}))
+    Xd, AXd = X.double(), AX.double()
+    cur = torch.cuda.current_stream()
+    ms2 = _time(lambda: (torch.mm(Xd, Xd.t()), torch.mm(Xd, AXd.t())), cur, a.reps)
+    print(json.dumps({"what": "cublas_fp64_same_contraction", "k": k, "rows": n, "ms": ms2,
+                      "tflops": 2 * 2.0 * n * k * k / ms2 / 1e9}))
+    M = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    ms3 = _time(lambda: torch.mm(M, M), cur, a.reps)
+    print(json.dumps({"what": "cublas_fp64_square_8192", "ms": ms3, "tflops": 2.0 * 8192 ** 3 / ms3 / 1e9}))
     return 0
 
 

@@ -198,3 +198,44 @@ def test_gram_blocks(cplx, prec, bdg):
     refs = [Su.conj() @ Su.T, Sv.conj() @ Sv.T, Su.conj() @ Sv.T, S.conj() @ AS.T]
     for g, r in zip(G, refs):
         assert relerr(g, r) < 1e-12
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_gram_blocks_streamk_vs_split(cplx, bdg, monkeypatch):
+    """The stream-K Gram schedule (default) against numpy and against the
+    row-split schedule (BDG_GRAM_SPLIT=1): k = 150 columns (three 64-wide
+    tiles, sym and non-sym tasks), an odd half length (padded tile rows, tasks
+    over n and over n/2 rows on one work line)."""
+    torch = _torch()
+    import bdg_lobpcg_b200 as B
+
+    rng = np.random.default_rng(8)
+    half, k = 40001, 150
+    n = 2 * half
+    S = rng.standard_normal((k, n))
+    AS = rng.standard_normal((k, n))
+    if cplx:
+        S = S + 1j * rng.standard_normal((k, n))
+        AS = AS + 1j * rng.standard_normal((k, n))
+    tdt = torch.complex128 if cplx else torch.float64
+    St = torch.tensor(S).to(tdt).cuda()
+    At = torch.tensor(AS).to(tdt).cuda()
+    dc = B.DeviceContext(1, [64], [1.0], cplx)  # the Gram does not depend on the grid
+    outs = []
+    for split in (False, True):
+        if split:
+            monkeypatch.setenv("BDG_GRAM_SPLIT", "1")
+        out = torch.full((4 * k * k * (2 if cplx else 1),), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        dc.gram_ptr(0, cplx, half, k, St.data_ptr(), n, At.data_ptr(), n, out.data_ptr())
+        dc.synchronize()
+        o = out.cpu().numpy()
+        if cplx:
+            o = o.view(np.complex128)
+        outs.append(o.reshape(4, k, k).transpose(0, 2, 1))
+    Su, Sv = S[:, :half], S[:, half:]
+    refs = [Su.conj() @ Su.T, Sv.conj() @ Sv.T, Su.conj() @ Sv.T, S.conj() @ AS.T]
+    for g, g2, r in zip(outs[0], outs[1], refs):
+        assert np.all(np.isfinite(g))
+        assert relerr(g, r) < 1e-12
+        assert relerr(g, g2) < 1e-13
