@@ -139,6 +139,26 @@ def lib():
         "bdgd_apply": (i, [vp, i, i, vp, u64, vp, u64, u64]),
         "bdgd_apply_host": (i, [vp, i, vp, vp, u64]),
         "bdgd_gram": (i, [vp, i, i, u64, u64, vp, u64, vp, u64, vp]),
+        "bdg_lp_create": (i, [C.POINTER(vp), _u64p, i, i, i]),
+        "bdg_lp_free": (None, [C.POINTER(vp)]),
+        "bdg_lp_nparams": (u64, [vp]),
+        "bdg_lp_get_params": (i, [vp, i, vp]),
+        "bdg_lp_set_params": (i, [vp, i, vp]),
+        "bdg_lp_init_random": (i, [vp, d, u64]),
+        "bdg_lp_save": (i, [vp, C.c_char_p]),
+        "bdg_lp_load": (i, [vp, C.c_char_p]),
+        "bdg_lp_condition": (i, [vp, _dp, _dp, d, d]),
+        "bdg_lp_regrid": (i, [vp, _u64p]),
+        "bdg_lp_apply_half": (i, [vp, vp, i, i, vp, u64, vp, u64, u64]),
+        "bdg_lp_apply": (i, [vp, vp, i, vp, u64, vp, u64, u64]),
+        "bdg_lp_loss_grad": (i, [vp, vp, i, vp, vp, vp, u64, u64, C.POINTER(d), vp]),
+        "bdg_lp_train_step": (i, [vp, vp, i, vp, vp, vp, u64, u64, d, C.POINTER(d)]),
+        "bdg_lp_cg": (i, [vp, i, d, vp, vp, u64, u64, d, i, C.POINTER(i)]),
+        "bdg_set_learned_precond": (i, [vp, vp, i]),
+        "bdg_learned_fallback_iteration": (C.c_int64, [vp]),
+        "bdg_set_residual_harvest": (i, [vp, vp, u64]),
+        "bdg_residual_harvest_count": (u64, [vp]),
+        "bdg_device_context": (vp, [vp]),
     }
     for name in ("kinetic", "matmulK", "matmulM", "matmulLrep", "matmulSwap", "precondK", "precondM",
                  "precondLrep", "dipolar_conv"):
@@ -400,6 +420,28 @@ class Problem:
     def set_goldstone_deflation(self, on):
         self._L.bdg_set_goldstone_deflation(self._h, 1 if on else 0)
 
+    def set_learned_precond(self, lp, stall_window=0):
+        rc = self._L.bdg_set_learned_precond(self._h, lp._p if lp is not None else None, stall_window)
+        if rc:
+            raise RuntimeError(f"bdg_set_learned_precond failed ({rc})")
+        self._keep.append(lp)
+
+    def learned_fallback_iteration(self):
+        return int(self._L.bdg_learned_fallback_iteration(self._h))
+
+    def set_residual_harvest(self, ptr, cap_cols):
+        self._L.bdg_set_residual_harvest(self._h, C.c_void_p(ptr) if ptr else None, cap_cols)
+
+    def residual_harvest_count(self):
+        return int(self._L.bdg_residual_harvest_count(self._h))
+
+    def device_context(self):
+        """The problem's own device context (operators uploaded), borrowed."""
+        p = self._L.bdg_device_context(self._h)
+        if not p:
+            raise RuntimeError("bdg_device_context failed: " + self._L.bdgd_last_error().decode())
+        return DeviceContext.borrow(p, self.size, self.cplx)
+
     def set_refinement(self, n):
         self._L.bdg_set_refinement(self._h, n)
 
@@ -480,8 +522,20 @@ class Problem:
 class DeviceContext:
     """bdgd_ctx: batched operator applies on device memory (bdg_cuda.h)."""
 
+    @classmethod
+    def borrow(cls, ptr, size, complex_psi0=False):
+        """Wrap a context owned by the library (e.g. bdg_device_context)."""
+        self = cls.__new__(cls)
+        self._L = lib()
+        self._c = C.c_void_p(ptr)
+        self._owned = False
+        self.cplx = bool(complex_psi0)
+        self.size = int(size)
+        return self
+
     def __init__(self, dim, N, L, complex_psi0=False):
         self._L = lib()
+        self._owned = True
         self._c = C.c_void_p()
         rc = self._L.bdgd_create(C.byref(self._c), dim, _c_arr(N, C.c_uint64), _c_arr(L, C.c_double),
                                  1 if complex_psi0 else 0)
@@ -494,14 +548,19 @@ class DeviceContext:
             raise RuntimeError(f"bdgd error {rc}: {self._L.bdgd_last_error().decode()}")
 
     def close(self):
-        if self._c:
+        if self._c and getattr(self, "_owned", True):
             self._L.bdgd_destroy(C.byref(self._c))
+        self._c = C.c_void_p()
 
     def __del__(self):
         try:
             self.close()
         except Exception:
             pass
+
+    @property
+    def ptr(self):
+        return self._c.value
 
     @property
     def stream(self):
@@ -536,3 +595,98 @@ class DeviceContext:
 
     def synchronize(self):
         self.check(self._L.bdgd_synchronize(self._c))
+
+
+# ---------------------------------------------------------------------------
+# learned SPD preconditioner (bdg/bdg_learn.h)
+# ---------------------------------------------------------------------------
+class LearnedPrecond:
+    """bdg_lp: T = S^T S + exp(eta) P0 per half; see include/bdg/bdg_learn.h."""
+
+    HALF_K, HALF_M = 0, 1
+
+    def __init__(self, N, C_=16, L=4, modes=12):
+        self._L = lib()
+        self._p = C.c_void_p()
+        self.N = list(N)
+        self.shape = (C_, L, modes)
+        self._check(self._L.bdg_lp_create(C.byref(self._p), _c_arr(N, C.c_uint64), C_, L, modes))
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(f"bdg_lp error {rc}: {self._L.bdgd_last_error().decode()}")
+
+    def close(self):
+        if self._p:
+            self._L.bdg_lp_free(C.byref(self._p))
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nparams(self):
+        return int(self._L.bdg_lp_nparams(self._p))
+
+    def get_params(self, half):
+        a = np.zeros(self.nparams, dtype=np.float32)
+        self._check(self._L.bdg_lp_get_params(self._p, half, _ptr(a)))
+        return a
+
+    def set_params(self, half, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        self._check(self._L.bdg_lp_set_params(self._p, half, _ptr(a)))
+
+    def init_random(self, amp, seed):
+        self._check(self._L.bdg_lp_init_random(self._p, amp, seed))
+
+    def save(self, path):
+        self._check(self._L.bdg_lp_save(self._p, str(path).encode()))
+
+    def load(self, path):
+        self._check(self._L.bdg_lp_load(self._p, str(path).encode()))
+
+    def condition(self, psi0, V, eps_dd, lam):
+        psi0 = np.ascontiguousarray(psi0, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        self._check(self._L.bdg_lp_condition(self._p, _dptr(psi0), _dptr(V), eps_dd, lam))
+
+    def regrid(self, N):
+        self.N = list(N)
+        self._check(self._L.bdg_lp_regrid(self._p, _c_arr(N, C.c_uint64)))
+
+    def apply_half_ptr(self, dev, half, prec, x_ptr, ldx, y_ptr, ldy, ncol):
+        self._check(self._L.bdg_lp_apply_half(self._p, C.c_void_p(dev.ptr), half, prec, C.c_void_p(x_ptr), ldx,
+                                              C.c_void_p(y_ptr), ldy, ncol))
+
+    def apply_ptr(self, dev, prec, x_ptr, ldx, y_ptr, ldy, ncol):
+        self._check(self._L.bdg_lp_apply(self._p, C.c_void_p(dev.ptr), prec, C.c_void_p(x_ptr), ldx,
+                                         C.c_void_p(y_ptr), ldy, ncol))
+
+    def loss_grad(self, dev, half, r_ptr, e_ptr, p0r_ptr, ld, ncol, want_grad=True):
+        loss = C.c_double()
+        g = np.zeros(self.nparams, dtype=np.float32) if want_grad else None
+        self._check(self._L.bdg_lp_loss_grad(self._p, C.c_void_p(dev.ptr), half, C.c_void_p(r_ptr),
+                                             C.c_void_p(e_ptr), C.c_void_p(p0r_ptr), ld, ncol, C.byref(loss),
+                                             _ptr(g) if want_grad else None))
+        return loss.value, g
+
+    def train_step(self, dev, half, r_ptr, e_ptr, p0r_ptr, ld, ncol, lr):
+        loss = C.c_double()
+        self._check(self._L.bdg_lp_train_step(self._p, C.c_void_p(dev.ptr), half, C.c_void_p(r_ptr),
+                                              C.c_void_p(e_ptr), C.c_void_p(p0r_ptr), ld, ncol, lr,
+                                              C.byref(loss)))
+        return loss.value
+
+
+def lp_cg(dev, op, sigma, r_ptr, e_ptr, ld, ncol, tol, maxit):
+    """e = (op + sigma)^-1 r on device columns (bdg_lp_cg); returns iterations."""
+    it = C.c_int()
+    rc = lib().bdg_lp_cg(C.c_void_p(dev.ptr), op, sigma, C.c_void_p(r_ptr), C.c_void_p(e_ptr), ld, ncol, tol,
+                         maxit, C.byref(it))
+    if rc:
+        raise RuntimeError(f"bdg_lp_cg error {rc}: {lib().bdgd_last_error().decode()}")
+    return it.value

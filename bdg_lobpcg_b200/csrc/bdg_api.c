@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "bdg/bdg_cuda.h"
+#include "bdg/bdg_learn.h"
 #include "bdg/bdg_internal.h"
 
 #ifndef M_PI
@@ -281,6 +282,37 @@ void bdg_set_goldstone_deflation(bdg_t *bdg, int enable) { bdg->deflate = enable
 void bdg_set_refinement(bdg_t *bdg, int max_iters) { bdg->refine_iters = max_iters < 0 ? 0 : max_iters; }
 
 const bdg_solve_stats_t *bdg_solve_stats(const bdg_t *bdg) { return &bdg->stats; }
+
+/* ---- learned preconditioner and residual harvesting (bdg/bdg_learn.h) ---- */
+int bdg_set_learned_precond(bdg_t *bdg, bdg_lp *lp, int stall_window) {
+  if (bdg == NULL) return -1;
+  if (bdg->complex_psi0 && lp != NULL) {
+    fprintf(stderr, "bdg_set_learned_precond: the learned preconditioner is for real (_d) problems\n");
+    return -2;
+  }
+  bdg->learned = lp;
+  bdg->learned_stall = stall_window > 0 ? stall_window : 12;
+  bdg->learned_fallback = -1;
+  return 0;
+}
+
+int64_t bdg_learned_fallback_iteration(const bdg_t *bdg) { return bdg ? bdg->learned_fallback : -1; }
+
+int bdg_set_residual_harvest(bdg_t *bdg, double *d_buf, uint64_t cap_cols) {
+  if (bdg == NULL) return -1;
+  bdg->harvest = d_buf;
+  bdg->harvest_cap = d_buf ? cap_cols : 0;
+  bdg->harvest_n = 0;
+  return 0;
+}
+
+uint64_t bdg_residual_harvest_count(const bdg_t *bdg) { return bdg ? bdg->harvest_n : 0; }
+
+bdgd_ctx *bdg_device_context(bdg_t *bdg) {
+  if (bdg == NULL || bdg->ctx == NULL) return NULL;
+  if (bdg_ctx_sync_device(bdg->ctx, BDGD_OP_LREP) || bdg_ctx_sync_device(bdg->ctx, BDGD_OP_TLREP)) return NULL;
+  return bdg->ctx->dev;
+}
 
 void bdg_set_trap_grid(bdg_t *bdg, const double *V) {
   BDG_REQUIRE(bdg, BDG_HAS_SYSTEM, "bdg_set_trap_grid");

@@ -40,6 +40,7 @@
 #include <time.h>
 
 #include "bdg/bdg_cuda.h"
+#include "bdg/bdg_learn.h"
 #include "bdg/bdg_internal.h"
 #include "bdg_blas.h"
 
@@ -638,6 +639,10 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   uint64_t it = 0;
   int nconv = 0;
   const int want_true = (o->criterion == BDG_CONV_TRUE_RESIDUAL);
+  /* learned preconditioner: on while the worst wanted residual keeps falling */
+  int use_learned = bdg->learned != NULL && !w->cplx && bdg->learned_fallback < 0;
+  const int stall_win = bdg->learned_stall > 0 ? bdg->learned_stall : 12;
+  double hist[256];
   for (;;) {
     cudaEventRecord(w->ev[3], st);
     TRY(measure(w, dev, o->anorm, lam, back, tres, want_true));
@@ -652,6 +657,17 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     }
     for (int j = nev; j < m; j++)
       if (back[j] > GUARD_LOCK) act[na++] = j;
+    if (use_learned) {
+      double wr = 0.0;
+      for (int j = 0; j < nev; j++) wr = fmax(wr, res_nev[j]);
+      hist[it % 256] = wr;
+      /* fall back to the plain preconditioner when the worst wanted residual
+       * has not fallen by 10% over the last stall_win iterations */
+      if (it >= (uint64_t)stall_win && stall_win < 256 && wr > 0.9 * hist[(it - stall_win) % 256]) {
+        use_learned = 0;
+        bdg->learned_fallback = (int64_t)it;
+      }
+    }
     if (nconv >= nev || it >= o->maxit) break;
     if (o->stop_backward_at_floor && worst <= o->floor) break;
     if (na == 0) break;
@@ -659,8 +675,23 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     CUDA_TRY(cudaMemcpyAsync(w->colmap, act, (size_t)na * sizeof(int), cudaMemcpyHostToDevice, st));
     DEV_TRY(bdgd_residual(dev, w->prec, w->cplx, w->S, (uint64_t)na, B(NB_X), B(NB_AX), w->n, B(NB_R), w->n,
                           w->lam_d, w->work, w->norms, w->norms + K, w->colmap));
+    if (bdg->harvest && w->prec == BDGD_F64 && !w->cplx && bdg->harvest_n < bdg->harvest_cap) {
+      /* residual columns for training a learned preconditioner */
+      uint64_t nh = bdg->harvest_cap - bdg->harvest_n;
+      if (nh > (uint64_t)na) nh = (uint64_t)na;
+      CUDA_TRY(cudaMemcpyAsync(bdg->harvest + bdg->harvest_n * w->n, B(NB_R), nh * w->n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+      bdg->harvest_n += nh;
+    }
     cudaEventRecord(w->ev[4], st);
     DEV_TRY(bdgd_apply(dev, BDGD_OP_TLREP, w->prec, B(NB_R), w->n, B(NB_WT), w->n, (uint64_t)na));
+    if (use_learned) {
+      /* learned T = S^T S + exp(eta) P0 on top of the plain apply P0 R */
+      const size_t eb = (w->prec == BDGD_F32 ? 4 : 8);
+      for (int h = 0; h < 2; ++h)
+        DEV_TRY(bdg_lp_apply_half((bdg_lp *)bdg->learned, dev, h, w->prec, (const char *)B(NB_R) + h * w->S * eb,
+                                  w->n, (char *)B(NB_WT) + h * w->S * eb, w->n, (uint64_t)na));
+    }
     cudaEventRecord(w->ev[5], st);
     TRY(deflate_block(w, dev, B(NB_WT), na));
     const int p = w->p;
@@ -789,6 +820,7 @@ static int solve_gpu(bdg_t *bdg) {
   const int cplx = bdg->complex_psi0;
   const uint64_t S = ctx->size, n = 2 * S, m = bdg->sizeSub, nev = bdg->nev;
   memset(&bdg->stats, 0, sizeof bdg->stats);
+  bdg->learned_fallback = -1;
   if (nev == 0 || m < nev || m > 1000) {
     fprintf(stderr, "bdg_solve: need 0 < nev <= sizeSub <= 1000\n");
     return -7;

@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from bdg_lobpcg_b200 import problems  # noqa: E402
+
 METRIC = "time to res<=1e-8, 32 BdG modes @128^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
@@ -47,68 +49,18 @@ def load_peaks():
 
 
 def problem_config(grid):
-    nev = {32: 8, 64: 16, 128: 32}.get(grid, 32)
-    L = 16.0 if grid == 32 else 24.0
-    eps = 0.5 if grid == 32 else 0.7
-    return dict(N=[grid] * 3, L=[L] * 3, omegas=(1.0, 1.0, 2.0), g=1000.0, gdd=1000.0 * eps, rc=8.0, nev=nev,
-                sizeSub=2 * nev, tol=1e-8, seed=0 if grid == 32 else 1)
+    return problems.config(grid)
 
 
-def grid_coords(N, L):
-    return [(np.arange(n) - 0.5 * n) * l / n for n, l in zip(N, L)]
-
-
-def trap(N, L, om):
-    x, y, z = grid_coords(N, L)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    return (0.5 * (om[0] ** 2 * X ** 2 + om[1] ** 2 * Y ** 2 + om[2] ** 2 * Z ** 2)).reshape(-1)
+grid_coords, trap = problems.grid_coords, problems.trap
 
 
 def ground_state(B, cfg):
-    """Stationary psi0 on the GPU (bdg_ground_state)."""
-    import ctypes as C
-
-    N, L = cfg["N"], cfg["L"]
-    x, y, z = grid_coords(N, L)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    psi = np.exp(-0.5 * (X * X + Y * Y + Z * Z)).reshape(-1).copy()
-    V = trap(N, L, cfg["omegas"])
-    lib = B.lib()
-    f = lib.bdg_ground_state
-    f.restype = C.c_int
-    f.argtypes = [C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_void_p, C.c_double, C.c_double,
-                  C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_void_p,
-                  C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
-    mu = C.c_double()
-    steps = C.c_uint64()
-    stat = C.c_double()
-    rc = f(3, (C.c_uint64 * 3)(*N), (C.c_double * 3)(*L), V.ctypes.data, cfg["g"], cfg["gdd"],
-           (C.c_double * 3)(0.0, 0.0, 1.0), cfg["rc"], 1e-3, 1e-12, 200000, 4, psi.ctypes.data, C.byref(mu),
-           C.byref(steps), C.byref(stat))
-    if rc:
-        raise RuntimeError(f"bdg_ground_state failed ({rc})")
-    return psi, mu.value, int(steps.value), stat.value, V
+    return problems.ground_state(B, cfg)
 
 
 def build(B, cfg, psi, mu, V, precision):
-    p = B.Problem(3, cfg["N"], cfg["L"])
-    p.set_system()
-    p.set_trap(V)
-    p.set_wavefunction(psi)
-    g = cfg["g"]
-    p.set_local_interactions(lambda n: g * n, lambda n: g * n)
-    p.set_dipolar(cfg["gdd"], [0.0, 0.0, 1.0], cfg["rc"])
-    p.set_mu(mu)
-    p.set_solver_params(cfg["nev"], cfg["sizeSub"], 2000, cfg["tol"])
-    p.set_convergence(B.CONV_TRUE_RESIDUAL)
-    p.set_goldstone_deflation(True)
-    p.set_precision(B.PREC_MIXED if precision == "mixed" else B.PREC_F64)
-    size = int(np.prod(cfg["N"]))
-    rng = np.random.default_rng(cfg["seed"])
-    u = rng.standard_normal((cfg["sizeSub"], size))
-    X0 = np.concatenate([u, u], axis=1)
-    p.set_initial_block(X0)
-    return p, X0
+    return problems.build(B, cfg, psi, mu, V, precision)
 
 
 class ClockSampler:

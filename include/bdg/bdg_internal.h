@@ -154,6 +154,12 @@ struct bdg_t {
   bdg_solve_stats_t stats;
   void *solver_ws;     /* cached device workspace of the GPU solver */
   void *block;         /* last solver block (host, n x sizeSub) */
+  /* learned preconditioner (bdg/bdg_learn.h) and residual harvesting */
+  void *learned;            /* struct bdg_lp *, or NULL for the plain preconditioner */
+  int learned_stall;        /* stall window (iterations) before the fallback */
+  int64_t learned_fallback; /* iteration of the last fallback, or -1 */
+  double *harvest;          /* device buffer of residual columns, or NULL */
+  uint64_t harvest_cap, harvest_n;
 };
 
 /* ---- context lifecycle (reference src/bdg_internal.h:151-153) ------------ */
