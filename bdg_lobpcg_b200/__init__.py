@@ -149,6 +149,8 @@ def lib():
         "bdg_lp_load": (i, [vp, C.c_char_p]),
         "bdg_lp_condition": (i, [vp, _dp, _dp, d, d]),
         "bdg_lp_regrid": (i, [vp, _u64p]),
+        "bdg_lp_set_energy_loss": (i, [vp, d]),
+        "bdg_lp_set_fast_math": (i, [vp, i]),
         "bdg_lp_apply_half": (i, [vp, vp, i, i, vp, u64, vp, u64, u64]),
         "bdg_lp_apply": (i, [vp, vp, i, vp, u64, vp, u64, u64]),
         "bdg_lp_loss_grad": (i, [vp, vp, i, vp, vp, vp, u64, u64, C.POINTER(d), vp]),
@@ -653,6 +655,14 @@ class LearnedPrecond:
         psi0 = np.ascontiguousarray(psi0, dtype=np.float64)
         V = np.ascontiguousarray(V, dtype=np.float64)
         self._check(self._L.bdg_lp_condition(self._p, _dptr(psi0), _dptr(V), eps_dd, lam))
+
+    def set_fast_math(self, on):
+        """Applies with TF32 tensor-core basis GEMMs (default) or exact FP32."""
+        self._check(self._L.bdg_lp_set_fast_math(self._p, 1 if on else 0))
+
+    def set_energy_loss(self, sigma):
+        """sigma >= 0: energy-norm loss of A = Op + sigma; sigma < 0: L2 loss."""
+        self._check(self._L.bdg_lp_set_energy_loss(self._p, sigma))
 
     def regrid(self, N):
         self.N = list(N)

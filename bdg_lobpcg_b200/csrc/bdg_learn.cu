@@ -11,6 +11,7 @@
 //   axis basis E_d   [R][n_d]: rows cos(2 pi a x/n), a < modes, then
 //                    sin(2 pi a x/n), 1 <= a < modes
 //   parameters       A [C][F] | W [L][C][M][M][M] | B [L][C][C] | Dg [L][C][F] | eta
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -42,8 +43,13 @@ struct bdg_lp {
   long long wsB;
   int wsTrain;
   float *rc[2], *acts[2], *gbuf[2], *sbuf, *co[2], *ax1, *ax2, *part;
-  double *tr, *dots, *fac;
+  double *tr, *tq, *dots, *fac;
   long long part_n;
+  // loss: L2 (energy = 0) or the energy norm of A = Op + esigma (energy = 1)
+  int energy;
+  double esigma;
+  cublasHandle_t blas;  // axis contractions of the spectral convolutions (plain FP32 GEMMs)
+  int fast;             // applies use TF32 tensor-core GEMMs (training always exact FP32)
 };
 
 // ---------------------------------------------------------------------------
@@ -126,26 +132,6 @@ __global__ void k_lp_lift_adj(const float *__restrict__ g, const float *__restri
   }
 }
 
-// out[o][i][q] = sum_m Mat(i, m) in[o][m][q], Mat(i, m) = E[i][m] (forward,
-// i < R, m < n) or E[m][i] (adjoint, i < n, m < R); E row length n.
-__global__ void k_lp_axis(const float *__restrict__ in, float *__restrict__ out, const float *__restrict__ E,
-                          long long outer, int lin, int lout, long long inner, int n, int adj) {
-  GSTRIDE(idx, outer * lout * inner) {
-    const long long q = idx % inner, t = idx / inner;
-    const int i = (int)(t % lout);
-    const long long o = t / lout;
-    const float *src = in + o * lin * inner + q;
-    float acc = 0.f;
-    if (adj) {
-      for (int m = 0; m < lin; ++m) acc += E[m * n + i] * src[m * inner];
-    } else {
-      const float *er = E + (long long)i * n;
-      for (int m = 0; m < lin; ++m) acc += er[m] * src[m * inner];
-    }
-    out[idx] = acc;
-  }
-}
-
 // co *= w_l[c] (filter of one layer, W = this layer's [C][M][M][M])
 __global__ void k_lp_filter(float *__restrict__ co, const float *__restrict__ W, int B, int C, int R, int M,
                             float inv_nc) {
@@ -190,30 +176,60 @@ __global__ void k_lp_filter_grad(const float *__restrict__ pz, const float *__re
 }
 
 // out = z + s + PM(z)  (transpose: PM^T), PM(z)[c] = sum_c' Bm[c][c'] z[c'] + (sum_f Dg[c][f] phi_f) z[c]
-__global__ void k_lp_layer(const float *__restrict__ z, const float *__restrict__ s, float *__restrict__ out,
-                           const float *__restrict__ Bm, const float *__restrict__ Dg, const float *__restrict__ phi,
-                           int B, int C, long long nc, int transpose) {
+// C is a compile-time channel count (the channel values stay in registers);
+// the layer's mix weights are staged in shared memory.
+template <int C>
+__global__ void __launch_bounds__(256) k_lp_layer(const float *__restrict__ z, const float *__restrict__ s,
+                                                  float *__restrict__ out, const float *__restrict__ Bm,
+                                                  const float *__restrict__ Dg, const float *__restrict__ phi, int B,
+                                                  long long nc, int transpose) {
+  __shared__ float sB[C * C], sD[C * LP_F];
+  for (int i = threadIdx.x; i < C * C; i += blockDim.x) {
+    const int r = i / C, q = i - r * C;
+    sB[i] = transpose ? Bm[q * C + r] : Bm[i];
+  }
+  for (int i = threadIdx.x; i < C * LP_F; i += blockDim.x) sD[i] = Dg[i];
+  __syncthreads();
   GSTRIDE(i, (long long)B * nc) {
     const long long b = i / nc, p = i - b * nc;
-    float zc[LP_CMAX];
-    float ph[LP_F];
+    const float *zb = z + b * C * nc + p;
+    float ph[LP_F], acc[C];
 #pragma unroll
     for (int f = 0; f < LP_F; ++f) ph[f] = phi[f * nc + p];
 #pragma unroll
-    for (int c = 0; c < LP_CMAX; ++c) zc[c] = c < C ? z[(b * C + c) * nc + p] : 0.f;
+    for (int c = 0; c < C; ++c) acc[c] = s[(b * C + c) * nc + p];
+    // one input channel at a time: acc[c] += B[c][c2] z[c2], plus the
+    // identity and conditioned diagonal on c = c2
+#pragma unroll 2
+    for (int c2 = 0; c2 < C; ++c2) {
+      const float zv = zb[(long long)c2 * nc];
+      float d = 1.f;
 #pragma unroll
-    for (int c = 0; c < LP_CMAX; ++c) {
-      if (c >= C) break;
-      float d = 0.f;
+      for (int f = 0; f < LP_F; ++f) d += sD[c2 * LP_F + f] * ph[f];
 #pragma unroll
-      for (int f = 0; f < LP_F; ++f) d += Dg[c * LP_F + f] * ph[f];
-      float acc = zc[c] + s[(b * C + c) * nc + p] + d * zc[c];
-#pragma unroll
-      for (int c2 = 0; c2 < LP_CMAX; ++c2)
-        if (c2 < C) acc += (transpose ? Bm[c2 * C + c] : Bm[c * C + c2]) * zc[c2];
-      out[(b * C + c) * nc + p] = acc;
+      for (int c = 0; c < C; ++c) acc[c] += (sB[c * C + c2] + (c == c2 ? d : 0.f)) * zv;
     }
+#pragma unroll
+    for (int c = 0; c < C; ++c) out[(b * C + c) * nc + p] = acc[c];
   }
+}
+
+// launch k_lp_layer for the channel counts the library builds (1, 2, 4, 8, 16)
+static int lp_layer_launch(cudaStream_t st, int C, const float *z, const float *s, float *out, const float *Bm,
+                           const float *Dg, const float *phi, int B, long long nc, int transpose) {
+  const unsigned nb = lp_blocks((long long)B * nc);
+  switch (C) {
+    case 1: k_lp_layer<1><<<nb, 256, 0, st>>>(z, s, out, Bm, Dg, phi, B, nc, transpose); break;
+    case 2: k_lp_layer<2><<<nb, 256, 0, st>>>(z, s, out, Bm, Dg, phi, B, nc, transpose); break;
+    case 4: k_lp_layer<4><<<nb, 256, 0, st>>>(z, s, out, Bm, Dg, phi, B, nc, transpose); break;
+    case 8: k_lp_layer<8><<<nb, 256, 0, st>>>(z, s, out, Bm, Dg, phi, B, nc, transpose); break;
+    case 16: k_lp_layer<16><<<nb, 256, 0, st>>>(z, s, out, Bm, Dg, phi, B, nc, transpose); break;
+    default:
+      bdgd_set_error("bdg_lp: channel count %d not built (1, 2, 4, 8 or 16)", C);
+      return BDGD_ERR_UNSUPPORTED;
+  }
+  bdgd_count_launch();
+  return BDGD_OK;
 }
 
 // Partial sums (block per (row c, split)) of
@@ -286,12 +302,12 @@ __global__ void k_lp_scale_cols(float *__restrict__ a, const double *__restrict_
 }
 
 // per column: dd = d.d, ee = e.e, dp = d.p0r (one block per column)
-__global__ void k_lp_coldots(const double *__restrict__ d, const double *__restrict__ e, const double *__restrict__ p,
-                             long long ld, long long S, double *__restrict__ out) {
+__global__ void k_lp_coldots(const double *__restrict__ d, long long ldd, const double *__restrict__ e,
+                             const double *__restrict__ p, long long ld, long long S, double *__restrict__ out) {
   const int b = blockIdx.x;
   double a0 = 0, a1 = 0, a2 = 0;
   for (long long i = threadIdx.x; i < S; i += blockDim.x) {
-    const double dv = d[b * ld + i], ev = e[b * ld + i], pv = p[b * ld + i];
+    const double dv = d[b * ldd + i], ev = e[b * ld + i], pv = p[b * ld + i];
     a0 += dv * dv;
     a1 += ev * ev;
     a2 += dv * pv;
@@ -313,6 +329,40 @@ __global__ void k_lp_coldots(const double *__restrict__ d, const double *__restr
     double v = 0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += red[threadIdx.x][k];
     out[b * 3 + threadIdx.x] = v;
+  }
+}
+
+// Energy loss terms per column, with q = A T r (Op applied, shift added here):
+// a0 = <Tr, q>, a1 = <r, Tr>, a2 = <r, e>; then q <- d = q - r and
+// a3 = <d, P0 r>.  tr, q leading dim S; r, e, p leading dim ld.
+__global__ void k_lp_edots(const double *__restrict__ tr, double *__restrict__ q, const double *__restrict__ r,
+                           const double *__restrict__ e, const double *__restrict__ p, double sigma, long long ld,
+                           long long S, double *__restrict__ out) {
+  const int b = blockIdx.x;
+  double a[4] = {0, 0, 0, 0};
+  for (long long i = threadIdx.x; i < S; i += blockDim.x) {
+    const double t = tr[b * S + i], rv = r[b * ld + i];
+    const double qv = q[b * S + i] + sigma * t;
+    a[0] += t * qv;
+    a[1] += rv * t;
+    a[2] += rv * e[b * ld + i];
+    const double dv = qv - rv;
+    q[b * S + i] = dv;
+    a[3] += dv * p[b * ld + i];
+  }
+  __shared__ double red[4][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double v = a[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += red[threadIdx.x][k];
+    out[b * 4 + threadIdx.x] = v;
   }
 }
 
@@ -362,12 +412,12 @@ static int lp_alloc(void **p, size_t bytes) {
 static void lp_free_ws(bdg_lp *lp) {
   void *bufs[] = {lp->rc[0], lp->rc[1], lp->acts[0], lp->acts[1], lp->gbuf[0], lp->gbuf[1], lp->sbuf,
                   lp->co[0], lp->co[1], lp->ax1,     lp->ax2,     lp->part,    lp->tr,      lp->dots,
-                  lp->fac};
+                  lp->fac,   lp->tq};
   for (void *b : bufs)
     if (b) cudaFree(b);
   lp->rc[0] = lp->rc[1] = lp->acts[0] = lp->acts[1] = lp->gbuf[0] = lp->gbuf[1] = lp->sbuf = nullptr;
   lp->co[0] = lp->co[1] = lp->ax1 = lp->ax2 = lp->part = nullptr;
-  lp->tr = lp->dots = lp->fac = nullptr;
+  lp->tr = lp->tq = lp->dots = lp->fac = nullptr;
   lp->wsB = 0;
   lp->wsTrain = 0;
 }
@@ -396,7 +446,8 @@ static int lp_workspace(bdg_lp *lp, long long B, int train) {
   if ((rc = lp_alloc((void **)&lp->part, sizeof(float) * lp->part_n))) return rc;
   if (train) {
     if ((rc = lp_alloc((void **)&lp->tr, sizeof(double) * B * lp->S))) return rc;
-    if ((rc = lp_alloc((void **)&lp->dots, sizeof(double) * B * 3))) return rc;
+    if ((rc = lp_alloc((void **)&lp->tq, sizeof(double) * B * lp->S))) return rc;
+    if ((rc = lp_alloc((void **)&lp->dots, sizeof(double) * B * 4))) return rc;
     if ((rc = lp_alloc((void **)&lp->fac, sizeof(double) * B))) return rc;
   }
   lp->wsB = B;
@@ -404,26 +455,48 @@ static int lp_workspace(bdg_lp *lp, long long B, int train) {
   return BDGD_OK;
 }
 
+// Contraction of the middle axis of in[outer][lin][inner] with the basis:
+// out[o][i][q] = sum_m Mat(i, m) in[o][m][q], Mat = E (forward, R x n) or
+// E^T (adjoint).  Plain FP32 GEMMs (cuBLAS, column-major view): one GEMM when
+// inner == 1, else one strided batch over `outer`.
+static int lp_axis(bdg_lp *lp, const float *in, float *out, const float *E, long long outer, int lin, int lout,
+                   long long inner, int n, int adj) {
+  const float one = 1.f, zero = 0.f;
+  cublasStatus_t st;
+  if (inner == 1) {
+    // C(lout x outer) = op(E_cm) (lout x lin) * in_cm (lin x outer)
+    st = cublasSgemm(lp->blas, adj ? CUBLAS_OP_N : CUBLAS_OP_T, CUBLAS_OP_N, lout, (int)outer, lin, &one, E, n, in,
+                     lin, &zero, out, lout);
+  } else {
+    // per o: C_o (inner x lout) = in_o (inner x lin) * op(E_cm) (lin x lout)
+    st = cublasSgemmStridedBatched(lp->blas, CUBLAS_OP_N, adj ? CUBLAS_OP_T : CUBLAS_OP_N, (int)inner, lout, lin, &one,
+                                   in, (int)inner, (long long)lin * inner, E, n, 0, &zero, out, (int)inner,
+                                   (long long)lout * inner, (int)outer);
+  }
+  if (st != CUBLAS_STATUS_SUCCESS) {
+    bdgd_set_error("bdg_lp: cuBLAS GEMM failed (%d)", (int)st);
+    return BDGD_ERR_CUDA;
+  }
+  bdgd_count_launch();
+  return BDGD_OK;
+}
+
 // coefficients co = P z for B*C fields
-static void lp_P(bdg_lp *lp, cudaStream_t st, const float *z, float *co, long long BC) {
+static int lp_P(bdg_lp *lp, const float *z, float *co, long long BC) {
   const int R = lp->R, n0 = lp->n[0], n1 = lp->n[1], n2 = lp->n[2];
-  long long o = BC * n2 * n1;
-  k_lp_axis<<<lp_blocks(o * R), 256, 0, st>>>(z, lp->ax1, lp->E[0], o, n0, R, 1, n0, 0);
-  o = BC * n2;
-  k_lp_axis<<<lp_blocks(o * R * R), 256, 0, st>>>(lp->ax1, lp->ax2, lp->E[1], o, n1, R, R, n1, 0);
-  k_lp_axis<<<lp_blocks(BC * R * R * R), 256, 0, st>>>(lp->ax2, co, lp->E[2], BC, n2, R, (long long)R * R, n2, 0);
-  for (int k = 0; k < 3; ++k) bdgd_count_launch();
+  int rc = lp_axis(lp, z, lp->ax1, lp->E[0], BC * n2 * n1, n0, R, 1, n0, 0);
+  if (!rc) rc = lp_axis(lp, lp->ax1, lp->ax2, lp->E[1], BC * n2, n1, R, R, n1, 0);
+  if (!rc) rc = lp_axis(lp, lp->ax2, co, lp->E[2], BC, n2, R, (long long)R * R, n2, 0);
+  return rc;
 }
 
 // z = P^T co
-static void lp_Pt(bdg_lp *lp, cudaStream_t st, const float *co, float *z, long long BC) {
+static int lp_Pt(bdg_lp *lp, const float *co, float *z, long long BC) {
   const int R = lp->R, n0 = lp->n[0], n1 = lp->n[1], n2 = lp->n[2];
-  k_lp_axis<<<lp_blocks(BC * n2 * R * R), 256, 0, st>>>(co, lp->ax2, lp->E[2], BC, R, n2, (long long)R * R, n2, 1);
-  long long o = BC * n2;
-  k_lp_axis<<<lp_blocks(o * n1 * R), 256, 0, st>>>(lp->ax2, lp->ax1, lp->E[1], o, R, n1, R, n1, 1);
-  o = BC * n2 * n1;
-  k_lp_axis<<<lp_blocks(o * n0), 256, 0, st>>>(lp->ax1, z, lp->E[0], o, R, n0, 1, n0, 1);
-  for (int k = 0; k < 3; ++k) bdgd_count_launch();
+  int rc = lp_axis(lp, co, lp->ax2, lp->E[2], BC, R, n2, (long long)R * R, n2, 1);
+  if (!rc) rc = lp_axis(lp, lp->ax2, lp->ax1, lp->E[1], BC * n2, R, n1, R, n1, 1);
+  if (!rc) rc = lp_axis(lp, lp->ax1, z, lp->E[0], BC * n2 * n1, R, n0, 1, n0, 1);
+  return rc;
 }
 
 static const float *lpW(bdg_lp *lp, int h, int l) { return lp->h[h].p + lp->oW + (long long)l * lp->C * lp->M * lp->M * lp->M; }
@@ -436,14 +509,15 @@ static int lp_layer(bdg_lp *lp, cudaStream_t st, int h, int l, int B, const floa
                     float *co) {
   const long long BC = (long long)B * lp->C;
   const float inv_nc = 1.0f / (float)lp->nc;
-  lp_P(lp, st, z, co, BC);
+  int rc = lp_P(lp, z, co, BC);
+  if (rc) return rc;
   k_lp_filter<<<lp_blocks(BC * lp->R * lp->R * lp->R), 256, 0, st>>>(co, lpW(lp, h, l), B, lp->C, lp->R, lp->M,
                                                                      inv_nc);
   bdgd_count_launch();
-  lp_Pt(lp, st, co, lp->sbuf, BC);
-  k_lp_layer<<<lp_blocks((long long)B * lp->nc), 256, 0, st>>>(z, lp->sbuf, out, lpB(lp, h, l), lpD(lp, h, l),
-                                                               lp->phi, B, lp->C, lp->nc, transpose);
-  bdgd_count_launch();
+  if ((rc = lp_Pt(lp, co, lp->sbuf, BC))) return rc;
+  if ((rc = lp_layer_launch(st, lp->C, z, lp->sbuf, out, lpB(lp, h, l), lpD(lp, h, l), lp->phi, B, lp->nc,
+                            transpose)))
+    return rc;
   LP_CK(cudaGetLastError());
   return BDGD_OK;
 }
@@ -490,8 +564,9 @@ static int lp_backprop(bdg_lp *lp, cudaStream_t st, int h, int B, const float *a
   float *gr = lp->h[h].g;
   for (int l = lp->L - 1; l >= 0; --l) {
     const float *z = acts + l * field;
-    lp_P(lp, st, z, lp->co[0], BC);
-    lp_P(lp, st, g, lp->co[1], BC);
+    int rc = lp_P(lp, z, lp->co[0], BC);
+    if (!rc) rc = lp_P(lp, g, lp->co[1], BC);
+    if (rc) return rc;
     k_lp_filter_grad<<<lp_blocks((long long)lp->C * lp->M * lp->M * lp->M), 256, 0, st>>>(
         lp->co[0], lp->co[1], gr + lp->oW + (long long)l * lp->C * lp->M * lp->M * lp->M, B, lp->C, lp->R, lp->M,
         inv_nc);
@@ -503,10 +578,10 @@ static int lp_backprop(bdg_lp *lp, cudaStream_t st, int h, int B, const float *a
     // g <- g + SC(g) + PM^T(g), reusing P g
     k_lp_filter<<<lp_blocks(BC * lp->R * lp->R * lp->R), 256, 0, st>>>(lp->co[1], lpW(lp, h, l), B, lp->C, lp->R,
                                                                        lp->M, inv_nc);
-    lp_Pt(lp, st, lp->co[1], lp->sbuf, BC);
-    k_lp_layer<<<lp_blocks((long long)B * lp->nc), 256, 0, st>>>(g, lp->sbuf, gn, lpB(lp, h, l), lpD(lp, h, l),
-                                                                 lp->phi, B, lp->C, lp->nc, 1);
-    for (int k = 0; k < 2; ++k) bdgd_count_launch();
+    if ((rc = lp_Pt(lp, lp->co[1], lp->sbuf, BC))) return rc;
+    if ((rc = lp_layer_launch(st, lp->C, g, lp->sbuf, gn, lpB(lp, h, l), lpD(lp, h, l), lp->phi, B, lp->nc, 1)))
+      return rc;
+    bdgd_count_launch();
     float *t = g;
     g = gn;
     gn = t;
@@ -565,11 +640,18 @@ static int lp_set_geometry(bdg_lp *lp, const uint64_t N[3]) {
 
 extern "C" int bdg_lp_create(bdg_lp **out, const uint64_t N[3], int C, int L, int modes) {
   *out = nullptr;
-  if (C < 1 || C > LP_CMAX || L < 1 || L > 16 || modes < 1) {
-    bdgd_set_error("bdg_lp_create: need 1 <= C <= %d, 1 <= L <= 16, modes >= 1", LP_CMAX);
+  if ((C != 1 && C != 2 && C != 4 && C != 8 && C != 16) || L < 1 || L > 16 || modes < 1) {
+    bdgd_set_error("bdg_lp_create: need C in {1, 2, 4, 8, 16}, 1 <= L <= 16, modes >= 1");
     return BDGD_ERR_ARG;
   }
   bdg_lp *lp = (bdg_lp *)calloc(1, sizeof(bdg_lp));
+  if (cublasCreate(&lp->blas) != CUBLAS_STATUS_SUCCESS) {
+    free(lp);
+    bdgd_set_error("bdg_lp_create: cublasCreate failed");
+    return BDGD_ERR_CUDA;
+  }
+  cublasSetMathMode(lp->blas, CUBLAS_PEDANTIC_MATH);  // true FP32 (no TF32 down-conversion)
+  lp->fast = 1;
   lp->C = C;
   lp->L = L;
   lp->M = modes;
@@ -609,6 +691,7 @@ extern "C" void bdg_lp_free(bdg_lp **plp) {
   for (int d = 0; d < 3; ++d)
     if (lp->E[d]) cudaFree(lp->E[d]);
   if (lp->phi) cudaFree(lp->phi);
+  if (lp->blas) cublasDestroy(lp->blas);
   for (int h = 0; h < 2; ++h) {
     cudaFree(lp->h[h].p);
     cudaFree(lp->h[h].g);
@@ -718,6 +801,19 @@ extern "C" int bdg_lp_load(bdg_lp *lp, const char *path) {
   return rc;
 }
 
+extern "C" int bdg_lp_set_fast_math(bdg_lp *lp, int on) {
+  if (!lp) return BDGD_ERR_ARG;
+  lp->fast = on ? 1 : 0;
+  return BDGD_OK;
+}
+
+extern "C" int bdg_lp_set_energy_loss(bdg_lp *lp, double sigma) {
+  if (!lp) return BDGD_ERR_ARG;
+  lp->energy = sigma >= 0.0;
+  lp->esigma = sigma >= 0.0 ? sigma : 0.0;
+  return BDGD_OK;
+}
+
 extern "C" int bdg_lp_regrid(bdg_lp *lp, const uint64_t N[3]) {
   if (!lp) return BDGD_ERR_ARG;
   return lp_set_geometry(lp, N);
@@ -772,6 +868,7 @@ extern "C" int bdg_lp_condition(bdg_lp *lp, const double *psi0, const double *V,
 
 static int lp_check(bdg_lp *lp, bdgd_ctx *dev) {
   if (!lp || !dev) return BDGD_ERR_ARG;
+  cublasSetStream(lp->blas, dev->stream);
   if (!lp->conditioned) {
     bdgd_set_error("bdg_lp: not conditioned (call bdg_lp_condition)");
     return BDGD_ERR_STATE;
@@ -791,6 +888,7 @@ extern "C" int bdg_lp_apply_half(bdg_lp *lp, bdgd_ctx *dev, int half, int prec, 
   if (rc) return rc;
   if (half < 0 || half > 1) return BDGD_ERR_ARG;
   cudaStream_t st = dev->stream;
+  cublasSetMathMode(lp->blas, lp->fast ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_PEDANTIC_MATH);
   for (uint64_t c0 = 0; c0 < ncol; c0 += kLpChunk) {
     const int B = (int)((ncol - c0) < (uint64_t)kLpChunk ? (ncol - c0) : kLpChunk);
     if ((rc = lp_workspace(lp, kLpChunk, lp->wsTrain))) return rc;
@@ -846,6 +944,7 @@ extern "C" int bdg_lp_loss_grad(bdg_lp *lp, bdgd_ctx *dev, int half, const doubl
   if (half < 0 || half > 1 || ncol == 0) return BDGD_ERR_ARG;
   if ((rc = lp_workspace(lp, (long long)ncol, 1))) return rc;
   cudaStream_t st = dev->stream;
+  cublasSetMathMode(lp->blas, CUBLAS_PEDANTIC_MATH);  // gradients in exact FP32
   const int B = (int)ncol;
   const long long S = lp->S, field = (long long)B * lp->C * lp->nc;
   LPHalf &H = lp->h[half];
@@ -861,13 +960,27 @@ extern "C" int bdg_lp_loss_grad(bdg_lp *lp, bdgd_ctx *dev, int half, const doubl
   k_lp_copy_cols<<<lp_blocks((long long)B * S), 256, 0, st>>>(d_p0r, (long long)ld, lp->tr, S, B, S);
   k_lp_poolt_axpy<double><<<lp_blocks((long long)B * S), 256, 0, st>>>(lp->rc[1], lp->tr, S, B, lp->N[0], lp->N[1],
                                                                        lp->N[2], H.p + lp->oEta);
-  k_lp_sub<<<lp_blocks((long long)B * S), 256, 0, st>>>(lp->tr, S, d_e, (long long)ld, B, S);
-  k_lp_coldots<<<B, 256, 0, st>>>(lp->tr, d_e, d_p0r, S, S, lp->dots);
-  for (int k = 0; k < 4; ++k) bdgd_count_launch();
+  const double *dvec;  // d of the gradient formula (leading dim S)
+  if (lp->energy) {
+    // q = Op T r (+ sigma T r in the dots kernel), d = q - r
+    if ((rc = bdgd_apply(dev, half ? BDGD_OP_M : BDGD_OP_K, BDGD_F64, lp->tr, (uint64_t)S, lp->tq, (uint64_t)S,
+                         (uint64_t)B)))
+      return rc;
+    k_lp_edots<<<B, 256, 0, st>>>(lp->tr, lp->tq, d_r, d_e, d_p0r, lp->esigma, (long long)ld, S, lp->dots);
+    bdgd_count_launch();
+    dvec = lp->tq;
+  } else {
+    k_lp_sub<<<lp_blocks((long long)B * S), 256, 0, st>>>(lp->tr, S, d_e, (long long)ld, B, S);
+    k_lp_coldots<<<B, 256, 0, st>>>(lp->tr, S, d_e, d_p0r, (long long)ld, S, lp->dots);
+    for (int k = 0; k < 2; ++k) bdgd_count_launch();
+    dvec = lp->tr;
+  }
+  for (int k = 0; k < 2; ++k) bdgd_count_launch();
   LP_CK(cudaGetLastError());
-  double *dots = (double *)malloc(sizeof(double) * B * 3), *fac = (double *)malloc(sizeof(double) * B);
+  const int nd = lp->energy ? 4 : 3;
+  double *dots = (double *)malloc(sizeof(double) * B * 4), *fac = (double *)malloc(sizeof(double) * B);
   float eta = 0.f;
-  cudaError_t e1 = cudaMemcpyAsync(dots, lp->dots, sizeof(double) * B * 3, cudaMemcpyDeviceToHost, st);
+  cudaError_t e1 = cudaMemcpyAsync(dots, lp->dots, sizeof(double) * B * nd, cudaMemcpyDeviceToHost, st);
   cudaError_t e2 = cudaMemcpyAsync(&eta, H.p + lp->oEta, sizeof(float), cudaMemcpyDeviceToHost, st);
   cudaError_t e3 = cudaStreamSynchronize(st);
   if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
@@ -877,10 +990,18 @@ extern "C" int bdg_lp_loss_grad(bdg_lp *lp, bdgd_ctx *dev, int half, const doubl
   }
   double loss = 0.0, geta = 0.0;
   for (int b = 0; b < B; ++b) {
-    const double ee = dots[b * 3 + 1] > 0 ? dots[b * 3 + 1] : 1e-300;
-    loss += dots[b * 3] / ee;
-    fac[b] = 2.0 / (ee * B);
-    geta += 2.0 * exp((double)eta) * dots[b * 3 + 2] / (ee * B);
+    if (lp->energy) {
+      const double *a = dots + b * 4;
+      const double re = a[2] > 0 ? a[2] : 1e-300;
+      loss += (a[0] - 2.0 * a[1] + a[2]) / re;
+      fac[b] = 2.0 / (re * B);
+      geta += 2.0 * exp((double)eta) * a[3] / (re * B);
+    } else {
+      const double ee = dots[b * 3 + 1] > 0 ? dots[b * 3 + 1] : 1e-300;
+      loss += dots[b * 3] / ee;
+      fac[b] = 2.0 / (ee * B);
+      geta += 2.0 * exp((double)eta) * dots[b * 3 + 2] / (ee * B);
+    }
   }
   loss /= B;
   if (loss_out) *loss_out = loss;
@@ -890,7 +1011,7 @@ extern "C" int bdg_lp_loss_grad(bdg_lp *lp, bdgd_ctx *dev, int half, const doubl
   free(fac);
   if (e4 != cudaSuccess || e5 != cudaSuccess) return bdgd_check(e4 != cudaSuccess ? e4 : e5, "bdg_lp_loss_grad");
   // forward S d (kept)
-  k_lp_pool<double><<<lp_blocks((long long)B * lp->nc), 256, 0, st>>>(lp->tr, S, B, lp->N[0], lp->N[1], lp->n[0],
+  k_lp_pool<double><<<lp_blocks((long long)B * lp->nc), 256, 0, st>>>(dvec, S, B, lp->N[0], lp->N[1], lp->n[0],
                                                                       lp->n[1], lp->n[2], lp->rc[1]);
   bdgd_count_launch();
   float *sd = lp_forward(lp, st, half, B, lp->rc[1], lp->acts[1], 1, &rc);

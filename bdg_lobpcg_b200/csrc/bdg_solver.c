@@ -658,12 +658,16 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     for (int j = nev; j < m; j++)
       if (back[j] > GUARD_LOCK) act[na++] = j;
     if (use_learned) {
+      /* the backward error (always evaluated; the true residual is gated) */
       double wr = 0.0;
-      for (int j = 0; j < nev; j++) wr = fmax(wr, res_nev[j]);
+      for (int j = 0; j < nev; j++)
+        if (!(back[j] <= wr)) wr = back[j]; /* NaN propagates */
       hist[it % 256] = wr;
       /* fall back to the plain preconditioner when the worst wanted residual
-       * has not fallen by 10% over the last stall_win iterations */
-      if (it >= (uint64_t)stall_win && stall_win < 256 && wr > 0.9 * hist[(it - stall_win) % 256]) {
+       * is not finite or has not fallen by 10% over the last stall_win
+       * iterations */
+      if (!isfinite(wr) ||
+          (it >= (uint64_t)stall_win && stall_win < 256 && !(wr <= 0.9 * hist[(it - stall_win) % 256]))) {
         use_learned = 0;
         bdg->learned_fallback = (int64_t)it;
       }

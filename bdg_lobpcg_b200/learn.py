@@ -5,12 +5,15 @@
 
 Pairs (r, e) come from the solver itself: the residual columns R = A X -
 lambda B X of plain FP64 solves are harvested on the device
-(bdg_set_residual_harvest); each half gives a pair for its network, with the
-target e = (K + sigma)^-1 r_u or (M + sigma)^-1 r_v from the library's inner
-CG (bdg_lp_cg) and P0 r from the plain preconditioner (T_K, T_M).  Columns
-are scaled to unit residual norm (the loss is scale invariant).  Training
-runs the library's forward / adjoint / gradient / Adam kernels
-(bdg_lp_train_step) on random batches.  torch only holds device buffers.
+(bdg_set_residual_harvest); each half gives a pair for its network, with
+e = (K + sigma)^-1 r_u or (M + sigma)^-1 r_v from the library's inner CG
+(bdg_lp_cg) and P0 r from the plain preconditioner (T_K, T_M).  Columns are
+scaled to unit residual norm (the loss is scale invariant).  The loss is the
+energy norm ||T r - e||_A^2 / ||e||_A^2 of A = Op + sigma (the norm in
+which a preconditioner's quality shows in the eigensolver; fitting e in
+the plain 2-norm made the solver slower).  Training runs the library's
+forward / adjoint / gradient / Adam kernels (bdg_lp_train_step) on random
+batches.  torch only holds device buffers.
 
 The sweep of the benchmark's learned-preconditioner configuration: 64^3
 problems in [-12, 12)^3 with eps_dd ~ U[0, 0.8], lambda ~ U[0.5, 3],
@@ -68,9 +71,12 @@ def make_pairs(B, p, cfg, psi, V, cap, sigma=1.0, cg_tol=1e-6, cg_maxit=400, max
     return out, iters
 
 
-def train(lp, dev, pairs, steps=300, batch=16, lr=1e-3, seed=0, log=None):
-    """Adam on random batches of the pairs of each half; returns the loss
-    history {half: [(step, loss), ...]}."""
+def train(lp, dev, pairs, steps=300, batch=16, lr=1e-3, seed=0, log=None, cosine=False, t0=0, total=None):
+    """Adam on random batches of the pairs of each half (cosine: learning
+    rate lr * (1 + cos(pi t / total)) / 2 at global step t = t0 + it, total
+    defaulting to steps); returns the loss history {half: [(step, loss)]}."""
+    import math
+
     torch = _torch()
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = {}
@@ -82,7 +88,9 @@ def train(lp, dev, pairs, steps=300, batch=16, lr=1e-3, seed=0, log=None):
             idx = torch.randint(0, ncol, (min(batch, ncol),), generator=g).cuda()
             rb, eb, pb = r[idx].contiguous(), e[idx].contiguous(), p0[idx].contiguous()
             torch.cuda.synchronize()
-            loss = lp.train_step(dev, half, rb.data_ptr(), eb.data_ptr(), pb.data_ptr(), S, rb.shape[0], lr)
+            T = total if total else steps
+            lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * min(t0 + it, T) / T)) if cosine else lr
+            loss = lp.train_step(dev, half, rb.data_ptr(), eb.data_ptr(), pb.data_ptr(), S, rb.shape[0], lr_t)
             hist[half].append((it, loss))
             if log and (it % 50 == 0 or it == steps - 1):
                 log(f"half {half} step {it} loss {loss:.5f}")
@@ -106,12 +114,12 @@ def eval_loss(lp, dev, pairs):
     return out
 
 
-def solve_with(B, cfg, psi, mu, V, lp=None, precision="f64"):
+def solve_with(B, cfg, psi, mu, V, lp=None, precision="f64", stall_window=0):
     """Fresh problem, same X0; returns (iterations, seconds, eigenvalues,
-    max true residual, fallback iteration)."""
+    max true residual, fallback iteration, device seconds)."""
     p, _ = problems.build(B, cfg, psi, mu, V, precision)
     if lp is not None:
-        p.set_learned_precond(lp)
+        p.set_learned_precond(lp, stall_window)
     t0 = time.perf_counter()
     rc = p.solve()
     t = time.perf_counter() - t0
@@ -142,8 +150,10 @@ def cmd_train(a):
             lp.init_random(a.init_amp, a.seed)
         pairs, iters = make_pairs(B, p, cfg, psi, V, a.cap, sigma=a.sigma)
         lp.condition(psi, V, eps, lam)
+        lp.set_energy_loss(a.sigma)
         dev = p.device_context()
-        hist = train(lp, dev, pairs, steps=a.steps, batch=a.batch, lr=a.lr, seed=k)
+        hist = train(lp, dev, pairs, steps=a.steps, batch=a.batch, lr=a.lr, seed=k, cosine=True, t0=k * a.steps,
+                     total=a.problems * a.steps)
         npairs += 2 * pairs[0][0].shape[0]
         print(json.dumps({"problem": k, "eps_dd": eps, "lambda": lam, "mu": mu, "harvest_iters": iters,
                           "pairs": 2 * pairs[0][0].shape[0], "loss_K": hist[0][-1][1], "loss_M": hist[1][-1][1],
@@ -185,11 +195,11 @@ def main(argv=None):
     t.add_argument("--problems", type=int, default=16)
     t.add_argument("--grid", type=int, default=64)
     t.add_argument("--nev", type=int, default=16)
-    t.add_argument("--cap", type=int, default=1024)
+    t.add_argument("--cap", type=int, default=512)
     t.add_argument("--harvest-iters", type=int, default=60)
-    t.add_argument("--steps", type=int, default=400)
+    t.add_argument("--steps", type=int, default=1000)
     t.add_argument("--batch", type=int, default=16)
-    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--lr", type=float, default=2e-3)
     t.add_argument("--sigma", type=float, default=1.0)
     t.add_argument("--init-amp", type=float, default=0.05)
     t.add_argument("--seed", type=int, default=4)

@@ -40,8 +40,8 @@ typedef struct bdg_lp bdg_lp;
 enum { BDG_LP_HALF_K = 0, BDG_LP_HALF_M = 1 };
 
 /* Create a preconditioner for the fine 3D grid N (even extents >= 8) with
- * channels C, layers L and retained wave numbers `modes` per axis (modes <=
- * N/4).  Parameters start at the plain preconditioner (S = 0, eta = 0).
+ * channels C (1, 2, 4, 8 or 16), layers L and retained wave numbers `modes`
+ * per axis (modes <= N/4).  Parameters start at the plain preconditioner (S = 0, eta = 0).
  * Returns 0 or a BDGD_ERR_* code (bdgd_last_error explains). */
 int bdg_lp_create(bdg_lp **out, const uint64_t N[3], int C, int L, int modes);
 void bdg_lp_free(bdg_lp **lp);
@@ -77,6 +77,12 @@ int bdg_lp_regrid(bdg_lp *lp, const uint64_t N[3]);
 int bdg_lp_apply_half(bdg_lp *lp, bdgd_ctx *dev, int half, int prec, const void *d_x, uint64_t ldx, void *d_y,
                       uint64_t ldy, uint64_t ncol);
 
+/* Applies run the basis contractions of the spectral convolutions as TF32
+ * tensor-core GEMMs (on = 1, the default; about 1e-3 relative error, ample
+ * for a preconditioner) or in exact FP32 (on = 0).  Training steps are
+ * always exact FP32. */
+int bdg_lp_set_fast_math(bdg_lp *lp, int on);
+
 /* Full T on [u; v] columns: y = T x with P0 = the plain T_Lrep of dev. */
 int bdg_lp_apply(bdg_lp *lp, bdgd_ctx *dev, int prec, const void *d_x, uint64_t ldx, void *d_y, uint64_t ldy,
                  uint64_t ncol);
@@ -86,6 +92,13 @@ int bdg_lp_apply(bdg_lp *lp, bdgd_ctx *dev, int prec, const void *d_x, uint64_t 
  * grad_out (host, nparams floats, may be NULL) the gradient of that mean. */
 int bdg_lp_loss_grad(bdg_lp *lp, bdgd_ctx *dev, int half, const double *d_r, const double *d_e,
                      const double *d_p0r, uint64_t ld, uint64_t ncol, double *loss_out, float *grad_out);
+
+/* Loss of bdg_lp_loss_grad / bdg_lp_train_step: sigma < 0 selects the L2
+ * loss above (the default); sigma >= 0 the energy norm
+ * ||T r - e||_A^2 / ||e||_A^2 of A = Op + sigma (Op = K for half 0, M for
+ * half 1, applied through the dev passed to those calls), which needs
+ * e = A^-1 r only in <r, e>. */
+int bdg_lp_set_energy_loss(bdg_lp *lp, double sigma);
 
 /* One Adam step (lr; beta1 0.9, beta2 0.999, eps 1e-8) of one half on ncol
  * pairs; loss_out (may be NULL) receives the loss before the step. */
@@ -102,8 +115,9 @@ int bdg_lp_cg(bdgd_ctx *dev, int op, double sigma, const double *d_r, double *d_
 /* Solver hooks (bdg_t of bdg.h). */
 /* Use lp as the preconditioner of bdg_solve (NULL: plain).  lp must be
  * conditioned on the same problem; the solver falls back to the plain
- * preconditioner for the rest of a solve when the worst wanted residual has
- * not fallen by 10% over `stall_window` iterations (0: 12). */
+ * preconditioner for the rest of a solve when the worst backward error of the
+ * wanted pairs is not finite or has not fallen by 10% over `stall_window`
+ * iterations (0: 12). */
 int bdg_set_learned_precond(bdg_t *bdg, bdg_lp *lp, int stall_window);
 /* Iteration at which the last solve fell back to the plain preconditioner,
  * or -1. */

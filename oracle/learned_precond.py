@@ -38,11 +38,11 @@ pointwise channel mix with a conditioned diagonal:
     PM_l(z)[c] = sum_c' B_l[c, c'] z[c'] + (sum_f Dg_l[c, f] phi_f) z[c].
 
 S^T applies the adjoints in reverse order; T is symmetric positive definite
-whenever P0 is.  Training minimises ||T r - e||^2 / ||e||^2 over pairs
-(r, e); with d = T r - e the gradient is
-
-    grad = 2 / ||e||^2 * grad_theta <S d, S r>   (d, r held fixed)
-         + d/d eta: 2 exp(eta) <d, P0 r> / ||e||^2.
+whenever P0 is.  Training minimises, over pairs (r, e), either ||T r - e||^2 / ||e||^2
+(with d = T r - e the gradient is 2 / ||e||^2 grad_theta <S d, S r>, d and
+r held fixed, and 2 exp(eta) <d, P0 r> / ||e||^2 for eta) or the energy
+norm ||T r - e||_A^2 / ||e||_A^2 with e = A^-1 r (loss_and_grad_energy:
+the same form with d = A T r - r and <r, e> in place of ||e||^2).
 """
 import numpy as np
 
@@ -220,6 +220,23 @@ class Net:
         g = (self.backprop(d, sr, phi) + self.backprop(r, sd, phi)) * (2.0 / ee)
         geta = 2.0 * np.exp(self.eta) * float(d @ p0r) / ee
         return loss, np.concatenate([g, [geta]])
+
+
+def loss_and_grad_energy(net, r, e, p0r, phi, aop):
+    """Energy-norm loss of one pair, ||T r - e||_A^2 / ||e||_A^2 with
+    e = A^-1 r, evaluated as (<Tr, A Tr> - 2 <r, Tr> + <r, e>) / <r, e>, and
+    its gradient: with d = A T r - r it is 2 / <r, e> grad <S d, S r> (d, r
+    held fixed) and 2 exp(eta) <d, P0 r> / <r, e> for eta.  aop(x) = A x."""
+    tr = net.apply(r, phi, p0r)
+    atr = aop(tr)
+    re = float(r @ e)
+    loss = (float(tr @ atr) - 2.0 * float(r @ tr) + re) / re
+    d = atr - r
+    sr = net.forward(r, phi)
+    sd = net.forward(d, phi)
+    g = (net.backprop(d, sr, phi) + net.backprop(r, sd, phi)) * (2.0 / re)
+    geta = 2.0 * np.exp(net.eta) * float(d @ p0r) / re
+    return loss, np.concatenate([g, [geta]])
 
 
 def adam(params, grad, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8):

@@ -103,3 +103,33 @@ def test_adam_reduces_loss():
         LP.adam(th, g / len(pairs), m, v, step, 0.02)
         net.set_flat(th)
     assert tot < 0.5 * first
+
+
+def test_energy_gradient_matches_finite_differences():
+    net, rng = _net(5)
+    phi = _phi(rng)
+    S = int(np.prod(N))
+    dA = 1.0 + rng.random(S)
+
+    def aop(x):  # SPD: positive diagonal plus a smoothing term
+        return dA * x + LP.pool_t(LP.pool(x, N), N)
+
+    r, p0r = rng.standard_normal(S), 0.5 * rng.standard_normal(S)
+    Am = np.stack([aop(c) for c in np.eye(S)], axis=1)
+    e = np.linalg.solve(Am, r)
+    loss, grad = LP.loss_and_grad_energy(net, r, e, p0r, phi, aop)
+    tr = net.apply(r, phi, p0r)
+    assert abs(loss - (tr - e) @ Am @ (tr - e) / (e @ Am @ e)) < 1e-9 * max(loss, 1.0)
+    theta = net.flat()
+    h = 1e-6
+    for i in rng.choice(theta.size, 30, replace=False).tolist() + [theta.size - 1]:
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h
+        tm[i] -= h
+        net.set_flat(tp)
+        lp_, _ = LP.loss_and_grad_energy(net, r, e, p0r, phi, aop)
+        net.set_flat(tm)
+        lm_, _ = LP.loss_and_grad_energy(net, r, e, p0r, phi, aop)
+        fd = (lp_ - lm_) / (2 * h)
+        assert abs(fd - grad[i]) < 1e-6 * max(1.0, abs(fd)), (i, fd, grad[i])
+    net.set_flat(theta)
