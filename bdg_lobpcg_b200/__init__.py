@@ -161,6 +161,11 @@ def lib():
         "bdg_set_residual_harvest": (i, [vp, vp, u64]),
         "bdg_residual_harvest_count": (u64, [vp]),
         "bdg_device_context": (vp, [vp]),
+        "bdg_solve_batch": (i, [C.POINTER(vp), i, i, i, C.POINTER(i), _dp]),
+        "bdg_release_device_memory": (None, [vp]),
+        "bdgd_set_graphs": (i, [vp, i]),
+        "bdgd_fft_tuning": (i, [vp, i, i, C.POINTER(i), C.POINTER(C.c_float)]),
+        "bdgd_trim": (i, [vp]),
     }
     for name in ("kinetic", "matmulK", "matmulM", "matmulLrep", "matmulSwap", "precondK", "precondM",
                  "precondLrep", "dipolar_conv"):
@@ -598,6 +603,16 @@ class DeviceContext:
     def synchronize(self):
         self.check(self._L.bdgd_synchronize(self._c))
 
+    def set_graphs(self, on):
+        self.check(self._L.bdgd_set_graphs(self._c, 1 if on else 0))
+
+    def fft_tuning(self, op, prec):
+        """(path, [ms_reg, ms_ct]) chosen by the autotuner; path 0 = not tuned."""
+        path = C.c_int()
+        ms = (C.c_float * 2)()
+        self.check(self._L.bdgd_fft_tuning(self._c, op, prec, C.byref(path), ms))
+        return path.value, [ms[0], ms[1]]
+
 
 # ---------------------------------------------------------------------------
 # learned SPD preconditioner (bdg/bdg_learn.h)
@@ -700,3 +715,13 @@ def lp_cg(dev, op, sigma, r_ptr, e_ptr, ld, ncol, tol, maxit):
     if rc:
         raise RuntimeError(f"bdg_lp_cg error {rc}: {lib().bdgd_last_error().decode()}")
     return it.value
+
+
+def solve_batch(problems, concurrency=8, graphs=True):
+    """bdg_solve_batch over Problem objects; returns (return codes, seconds)."""
+    n = len(problems)
+    arr = (C.c_void_p * n)(*[p._h.value for p in problems])
+    rcs = (C.c_int * n)()
+    secs = np.zeros(n)
+    lib().bdg_solve_batch(arr, n, concurrency, 1 if graphs else 0, rcs, _dptr(secs))
+    return [rcs[i] for i in range(n)], secs

@@ -72,7 +72,20 @@ struct bdgd_ctx {
   size_t spec_cap;  // max scratch bytes per apply chunk
   double kin_dt;
   double *ptab;     // (1/size) / safe_val(mu + k^2/2) per spectrum point, for the current mu
+  // FFT pass family per (operator, precision) chosen by the autotuner:
+  // 0 not tuned, 1 register lines, 2 compile-time shared-memory stages
+  signed char tune[16][2];
+  float tune_ms[16][2][2];
+  int force_path;   // set while the autotuner times one family
+  // CUDA graphs of operator applies (bdgd_set_graphs)
+  int graphs_on;
+  unsigned version; // bumped by every setter and scratch reallocation
+  struct bdgd_graph *graphs;
+  int ngraphs;
 };
+
+// launches inside a stream capture skip per-launch attribute calls
+extern thread_local int bdgd_capturing;
 
 int bdgd_run_internal(bdgd_ctx *c, int kind, const void *d_x, long long ldx, void *d_y, long long ldy, int ncol);
 

@@ -8,6 +8,16 @@
 
 #include "bdg_dev.h"
 
+// Opt a kernel in to sm bytes of dynamic shared memory; skipped while a
+// stream capture records the launches (the attribute is already set by the
+// uncaptured first run of the same apply).
+template <typename K>
+static inline int bdgd_smem_attr(K kern, size_t sm) {
+  if (bdgd_capturing) return BDGD_OK;
+  BDGD_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  return BDGD_OK;
+}
+
 // ---------------------------------------------------------------------------
 // complex helpers
 // ---------------------------------------------------------------------------

@@ -678,7 +678,7 @@ static size_t lines_smem() {
 // every launch that needs it).
 template <typename K>
 static int set_smem(K kern, size_t sm) {
-  if (sm > 48 * 1024) BDGD_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (sm > 48 * 1024) { const int _ra = bdgd_smem_attr(kern, sm); if (_ra) return _ra; }
   return BDGD_OK;
 }
 

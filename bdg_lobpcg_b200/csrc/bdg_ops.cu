@@ -31,6 +31,8 @@
 #include "bdg_kern.cuh"
 #include "bdg_lines.h"
 
+static void graphs_clear(bdgd_ctx *c);
+
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
@@ -51,7 +53,9 @@ int bdgd_check(cudaError_t e, const char *what) {
 extern "C" const char *bdgd_last_error(void) { return g_err; }
 
 static unsigned long long g_launches = 0;
+thread_local int bdgd_capturing = 0;
 void bdgd_count_launch(void) { __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+static void count_launches(unsigned long long n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
 extern "C" unsigned long long bdgd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 extern "C" int bdgd_device_count(void) {
@@ -718,6 +722,7 @@ extern "C" int bdgd_create(bdgd_ctx **out, uint64_t dim, const uint64_t *N, cons
   c->nxk = c->cplx ? c->N[0] : c->N[0] / 2 + 1;
   c->H = (long long)c->nxk * c->N[1] * c->N[2];
   c->spec_cap = (size_t)4 << 30;
+  c->graphs_on = getenv("BDG_GRAPHS") && atoi(getenv("BDG_GRAPHS")) != 0;
   if (const char *e = getenv("BDG_SPEC_CAP_MB")) c->spec_cap = (size_t)atoll(e) << 20;
   if (cudaGetDevice(&c->device) != cudaSuccess) {
     cudaGetLastError();
@@ -792,6 +797,7 @@ extern "C" void bdgd_destroy(bdgd_ctx **pc) {
   if (!pc || !*pc) return;
   bdgd_ctx *c = *pc;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  graphs_clear(c);
   for (int d = 0; d < 3; ++d) {
     cudaFree(c->d_roots64[d]);
     cudaFree(c->d_roots32[d]);
@@ -860,6 +866,7 @@ static int upload_pair(bdgd_ctx *c, double **d64, float **d32, const double *h, 
 }
 
 extern "C" int bdgd_set_local_terms(bdgd_ctx *c, const double *ltK, const double *ltM) {
+  c->version++;
   int rc;
   if (ltK && (rc = upload_pair(c, &c->ltK64, &c->ltK32, ltK, c->S))) return rc;
   if (ltM && (rc = upload_pair(c, &c->ltM64, &c->ltM32, ltM, c->S))) return rc;
@@ -867,6 +874,7 @@ extern "C" int bdgd_set_local_terms(bdgd_ctx *c, const double *ltK, const double
 }
 
 extern "C" int bdgd_set_precond(bdgd_ctx *c, const double *sK, const double *sM, double mu) {
+  c->version++;
   int rc;
   if (sK && (rc = upload_pair(c, &c->pK64, &c->pK32, sK, c->S))) return rc;
   if (sM && (rc = upload_pair(c, &c->pM64, &c->pM32, sM, c->S))) return rc;
@@ -876,6 +884,7 @@ extern "C" int bdgd_set_precond(bdgd_ctx *c, const double *sK, const double *sM,
 }
 
 extern "C" int bdgd_set_wavefunction(bdgd_ctx *c, const void *wf) {
+  c->version++;
   if (!wf) return BDGD_OK;
   const long long n = c->S * (c->cplx ? 2 : 1);
   double *d64 = (double *)c->wf64;
@@ -889,6 +898,7 @@ extern "C" int bdgd_set_wavefunction(bdgd_ctx *c, const void *wf) {
 }
 
 extern "C" int bdgd_set_dipolar(bdgd_ctx *c, const double *vdd, double g_ddi, int enabled) {
+  c->version++;
   c->g_ddi = g_ddi;
   c->dipolar = enabled && c->dim == 3;
   if (vdd) {
@@ -918,7 +928,7 @@ static int launch_row_fwd_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, co
   constexpr int LPG = (256 / NF) / ct_tpl(NX);
   const size_t sm = sizeof(C) * NF * LPG * ct_line(NX);
   if (sm > 48 * 1024)
-    BDGD_CK(cudaFuncSetAttribute(k_row_fwd_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    { const int _ra = bdgd_smem_attr(k_row_fwd_ct<T, CPLX, NX, NF>, sm); if (_ra) return _ra; }
   const int nrb = (c->geo.nrows + LPG - 1) / LPG;
   bdgd_count_launch();
   k_row_fwd_ct<T, CPLX, NX, NF><<<dim3(nrb, nc), 256, sm, c->stream>>>(c->geo, p, fd, x, ldx, spec, h);
@@ -933,7 +943,7 @@ static int launch_row_inv_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, co
   constexpr int LPG = (256 / NF) / ct_tpl(NX);
   const size_t sm = sizeof(C) * NF * LPG * ct_line(NX);
   if (sm > 48 * 1024)
-    BDGD_CK(cudaFuncSetAttribute(k_row_inv_ct<T, CPLX, NX, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    { const int _ra = bdgd_smem_attr(k_row_inv_ct<T, CPLX, NX, NF>, sm); if (_ra) return _ra; }
   const int nrb = (c->geo.nrows + LPG - 1) / LPG;
   bdgd_count_launch();
   k_row_inv_ct<T, CPLX, NX, NF><<<dim3(nrb, nc), 256, sm, c->stream>>>(c->geo, p, fd, spec, x, ldx, y, ldy, h);
@@ -948,7 +958,7 @@ static int launch_col_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typena
   constexpr int TX = 256 / ct_tpl(N);
   const size_t sm = sizeof(C) * TX * (ct_line(N) | 1);
   if (sm > 48 * 1024)
-    BDGD_CK(cudaFuncSetAttribute(k_col_pass_ct<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    { const int _ra = bdgd_smem_attr(k_col_pass_ct<T, N>, sm); if (_ra) return _ra; }
   const int ntx = (c->nxk + TX - 1) / TX;
   const int outer = (axis == 1) ? c->N[2] : c->N[1];
   bdgd_count_launch();
@@ -1003,7 +1013,7 @@ static int cols_ct(bdgd_ctx *c, const Prog &p, const FieldsDev &fd, typename Cx<
 // = reg | ct | generic overrides (BDG_GENERIC_FFT=1 is the same as generic).
 enum { FFT_PATH_REG = 0, FFT_PATH_CT = 1, FFT_PATH_GENERIC = 2 };
 static int fft_path(const bdgd_ctx *c) {
-  (void)c;
+  if (c->force_path) return c->force_path == 2 ? FFT_PATH_CT : FFT_PATH_REG;
   if (getenv("BDG_GENERIC_FFT")) return FFT_PATH_GENERIC;
   const char *e = getenv("BDG_FFT_PATH");
   if (e) {
@@ -1038,7 +1048,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
     int maxnf = p.nf[0] > p.nf[p.nh - 1] ? p.nf[0] : p.nf[p.nh - 1];
     size_t sm = sizeof(C) * 2 * maxnf * Nx;
     if (sm > 48 * 1024)
-      BDGD_CK(cudaFuncSetAttribute(k_row_fused1d<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      { const int _ra = bdgd_smem_attr(k_row_fused1d<T, CPLX>, sm); if (_ra) return _ra; }
     dim3 grid(1, ncol * p.nh);
     bdgd_count_launch();
     k_row_fused1d<T, CPLX><<<grid, kThreads, sm, c->stream>>>(g, p, fd, x, ldx, y, ldy);
@@ -1053,8 +1063,10 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
     if (chunk < 1) chunk = 1;
   }
   if (only_fwd || only_bwd) chunk = ncol;  // raw transforms use the whole scratch as I/O
+  void *spec_before = c->spec;
   int rc = bdgd_ensure(&c->spec, &c->spec_bytes, per_col * (size_t)chunk);
   if (rc) return rc;
+  if (c->spec != spec_before) c->version++;  // captured graphs hold the old scratch
   C *spec = (C *)c->spec;
   const int tx = f32 ? 16 : 8;
   if (!only_fwd && !only_bwd && fft_path(c) == FFT_PATH_REG && bdgd_lines_usable(c, p)) {
@@ -1100,7 +1112,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
     if (!only_bwd) {
       size_t sm = sizeof(C) * 2 * rpb * Nx;
       if (sm > 48 * 1024)
-        BDGD_CK(cudaFuncSetAttribute(k_row_fwd<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        { const int _ra = bdgd_smem_attr(k_row_fwd<T, CPLX>, sm); if (_ra) return _ra; }
       bdgd_count_launch();
       k_row_fwd<T, CPLX><<<dim3(nrb, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, xc, ldx, spec, rpb);
       BDGD_CK(cudaGetLastError());
@@ -1114,7 +1126,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       const int outer = (ax == 1) ? c->N[2] : c->N[1];
       size_t sm = sizeof(C) * 2 * tx * (n + 1);
       if (sm > 48 * 1024)
-        BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        { const int _ra = bdgd_smem_attr(k_col_pass<T>, sm); if (_ra) return _ra; }
       bdgd_count_launch();
       k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, mode, tx);
       BDGD_CK(cudaGetLastError());
@@ -1127,7 +1139,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       const int outer = (ax == 1) ? c->N[2] : c->N[1];
       size_t sm = sizeof(C) * 2 * tx * (n + 1);
       if (sm > 48 * 1024)
-        BDGD_CK(cudaFuncSetAttribute(k_col_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        { const int _ra = bdgd_smem_attr(k_col_pass<T>, sm); if (_ra) return _ra; }
       bdgd_count_launch();
       k_col_pass<T><<<dim3(ntx * outer, nc * p.J), kThreads, sm, c->stream>>>(g, p, fd, spec, ax, 1, tx);
       BDGD_CK(cudaGetLastError());
@@ -1137,7 +1149,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
       for (int h = 0; h < p.nh; ++h) maxnf = p.nf[h] > maxnf ? p.nf[h] : maxnf;
       size_t sm = sizeof(C) * 2 * maxnf * rpb * Nx;
       if (sm > 48 * 1024)
-        BDGD_CK(cudaFuncSetAttribute(k_row_inv<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        { const int _ra = bdgd_smem_attr(k_row_inv<T, CPLX>, sm); if (_ra) return _ra; }
       bdgd_count_launch();
       k_row_inv<T, CPLX><<<dim3(nrb, nc * p.nh), kThreads, sm, c->stream>>>(g, p, fd, spec, xc, ldx, yc, ldy, rpb);
       BDGD_CK(cudaGetLastError());
@@ -1179,6 +1191,173 @@ static int dispatch(bdgd_ctx *c, const Prog &p, int prec, const void *x, long lo
   return run_program<double, false>(c, p, x, ldx, y, ldy, ncol, only_fwd, only_bwd);
 }
 
+// ---------------------------------------------------------------------------
+// CUDA graphs of operator applies and the FFT pass-family autotuner
+// ---------------------------------------------------------------------------
+struct bdgd_graph {
+  int op, prec, ncol, path;
+  const void *x;
+  void *y;
+  long long ldx, ldy;
+  unsigned version;
+  cudaGraphExec_t exec;  // null after the first (uncaptured) use
+  unsigned long long nkern, stamp;
+};
+#define BDGD_MAX_GRAPHS 48
+static unsigned long long g_graph_clock = 0;
+
+static void graphs_clear(bdgd_ctx *c) {
+  for (int i = 0; i < c->ngraphs; ++i)
+    if (c->graphs[i].exec) cudaGraphExecDestroy(c->graphs[i].exec);
+  free(c->graphs);
+  c->graphs = nullptr;
+  c->ngraphs = 0;
+}
+
+extern "C" int bdgd_trim(bdgd_ctx *c) {
+  if (!c) return BDGD_ERR_ARG;
+  BDGD_CK(cudaStreamSynchronize(c->stream));
+  graphs_clear(c);
+  void **bufs[] = {&c->spec, &c->io, (void **)&c->gram_part};
+  size_t *sizes[] = {&c->spec_bytes, &c->io_bytes, &c->gram_part_bytes};
+  for (int i = 0; i < 3; ++i) {
+    if (*bufs[i]) cudaFree(*bufs[i]);
+    *bufs[i] = nullptr;
+    *sizes[i] = 0;
+  }
+  c->version++;
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_set_graphs(bdgd_ctx *c, int on) {
+  if (!c) return BDGD_ERR_ARG;
+  c->graphs_on = on ? 1 : 0;
+  if (!on) graphs_clear(c);
+  return BDGD_OK;
+}
+
+extern "C" int bdgd_fft_tuning(bdgd_ctx *c, int op, int prec, int *path_out, float *ms_out) {
+  if (!c || op < 0 || op >= 16) return BDGD_ERR_ARG;
+  const int pi = prec == BDGD_F32 ? 1 : 0;
+  if (path_out) *path_out = c->tune[op][pi];
+  if (ms_out) {
+    ms_out[0] = c->tune_ms[op][pi][0];
+    ms_out[1] = c->tune_ms[op][pi][1];
+  }
+  return BDGD_OK;
+}
+
+// Run one apply through a cached graph: the first use of a key runs
+// uncaptured (allocations, attributes), the second captures and launches
+// the graph, later uses replay it.  Keys include the context version, which
+// every setter and scratch reallocation bumps.
+static int apply_graph(bdgd_ctx *c, int op, const Prog &p, int prec, const void *x, long long ldx, void *y,
+                       long long ldy, int ncol) {
+  bdgd_graph *g = nullptr;
+  for (int i = 0; i < c->ngraphs; ++i) {
+    bdgd_graph &e = c->graphs[i];
+    if (e.op == op && e.prec == prec && e.ncol == ncol && e.x == x && e.y == y && e.ldx == ldx && e.ldy == ldy &&
+        e.path == c->force_path && e.version == c->version) {
+      g = &e;
+      break;
+    }
+  }
+  if (g && g->exec) {
+    g->stamp = ++g_graph_clock;
+    BDGD_CK(cudaGraphLaunch(g->exec, c->stream));
+    count_launches(g->nkern);
+    return BDGD_OK;
+  }
+  if (!g) {
+    if (!c->graphs) c->graphs = (bdgd_graph *)calloc(BDGD_MAX_GRAPHS, sizeof(bdgd_graph));
+    if (c->ngraphs < BDGD_MAX_GRAPHS) {
+      g = &c->graphs[c->ngraphs++];
+    } else {  // replace the least recently used entry
+      g = &c->graphs[0];
+      for (int i = 1; i < c->ngraphs; ++i)
+        if (c->graphs[i].stamp < g->stamp) g = &c->graphs[i];
+      if (g->exec) cudaGraphExecDestroy(g->exec);
+    }
+    memset(g, 0, sizeof *g);
+    g->op = op;
+    g->prec = prec;
+    g->ncol = ncol;
+    g->x = x;
+    g->y = y;
+    g->ldx = ldx;
+    g->ldy = ldy;
+    g->path = c->force_path;
+    g->version = c->version;
+    g->stamp = ++g_graph_clock;
+    return dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+  }
+  // second use: capture
+  const unsigned long long l0 = bdgd_launch_count();
+  cudaGraph_t gr = nullptr;
+  BDGD_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  bdgd_capturing = 1;
+  int rc = dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+  bdgd_capturing = 0;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+  const unsigned long long nk = bdgd_launch_count() - l0;
+  cudaGraphExec_t ex = nullptr;
+  if (!rc && e == cudaSuccess && gr) e = cudaGraphInstantiate(&ex, gr, 0);
+  if (gr) cudaGraphDestroy(gr);
+  if (rc || e != cudaSuccess || !ex) {
+    // not capturable here: run it directly (nothing of the capture ran)
+    cudaGetLastError();
+    __atomic_sub_fetch(&g_launches, nk, __ATOMIC_RELAXED);
+    g->version = c->version - 1;  // never matches again
+    return dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+  }
+  g->exec = ex;
+  g->nkern = nk;
+  BDGD_CK(cudaGraphLaunch(ex, c->stream));  // the recorded launches are counted already
+  return BDGD_OK;
+}
+
+// Choose the FFT pass family of (op, prec) on this context by timing both
+// (each run twice, the second timed) on its first apply of >= 4 columns;
+// later applies use the faster one.  BDG_FFT_PATH / BDG_GENERIC_FFT override.
+static int apply_tuned(bdgd_ctx *c, int op, const Prog &p, int prec, const void *x, long long ldx, void *y,
+                       long long ldy, int ncol) {
+  const int pi = prec == BDGD_F32 ? 1 : 0;
+  const bool env = getenv("BDG_FFT_PATH") || getenv("BDG_GENERIC_FFT");
+  const bool tunable = !env && bdgd_lines_usable(c, p) && op < 16;
+  if (tunable && c->tune[op][pi] == 0 && ncol >= 4 && !bdgd_capturing) {
+    float ms[2] = {0.f, 0.f};
+    cudaEvent_t e0, e1;
+    BDGD_CK(cudaEventCreate(&e0));
+    BDGD_CK(cudaEventCreate(&e1));
+    int rc = BDGD_OK;
+    for (int k = 0; k < 2 && !rc; ++k) {
+      c->force_path = k + 1;
+      rc = dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+      if (!rc) {
+        cudaEventRecord(e0, c->stream);
+        rc = dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+        cudaEventRecord(e1, c->stream);
+        cudaError_t ce = cudaEventSynchronize(e1);
+        if (ce != cudaSuccess) rc = bdgd_check(ce, "autotune");
+        else cudaEventElapsedTime(&ms[k], e0, e1);
+      }
+    }
+    c->force_path = 0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    c->tune[op][pi] = ms[0] <= ms[1] ? 1 : 2;
+    c->tune_ms[op][pi][0] = ms[0];
+    c->tune_ms[op][pi][1] = ms[1];
+    return BDGD_OK;  // y holds the result of the last run
+  }
+  if (tunable && c->tune[op][pi]) c->force_path = c->tune[op][pi];
+  const int rc = (c->graphs_on && !bdgd_capturing) ? apply_graph(c, op, p, prec, x, ldx, y, ldy, ncol)
+                                                   : dispatch(c, p, prec, x, ldx, y, ldy, ncol, 0, 0);
+  c->force_path = 0;
+  return rc;
+}
+
 extern "C" int bdgd_apply(bdgd_ctx *c, int op, int prec, const void *d_x, uint64_t ldx, void *d_y, uint64_t ldy,
                           uint64_t ncol) {
   if (!c || !d_x || !d_y) {
@@ -1215,7 +1394,7 @@ extern "C" int bdgd_apply(bdgd_ctx *c, int op, int prec, const void *d_x, uint64
     return BDGD_ERR_ARG;
   }
   Prog p = make_prog(op, c->dipolar && c->dim == 3);
-  return dispatch(c, p, prec, d_x, (long long)ldx, d_y, (long long)ldy, (int)ncol, 0, 0);
+  return apply_tuned(c, op, p, prec, d_x, (long long)ldx, d_y, (long long)ldy, (int)ncol);
 }
 
 extern "C" int bdgd_apply_host(bdgd_ctx *c, int op, const void *x, void *y, uint64_t ncol) {

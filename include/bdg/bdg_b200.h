@@ -79,6 +79,21 @@ int bdg_ground_state(uint64_t dim, const uint64_t *N, const double *L, const dou
                      int newton_steps, double *psi_inout, double *mu_out, uint64_t *steps_out,
                      double *stationarity_out);
 
+/* Solve n independent, fully set-up problems on one GPU (no counterpart in
+ * the reference, which solves one problem per call).  Up to `concurrency`
+ * solves run at once, each on its own host thread and CUDA stream; with
+ * `graphs` set their operator applies replay CUDA graphs (bdgd_set_graphs).
+ * After each solve the problem's device workspace is released
+ * (bdg_release_device_memory); results stay in the problem.  rcs_out[i]
+ * (may be NULL) receives bdg_solve's return code, seconds_out[i] (may be
+ * NULL) the wall time of that solve.  Returns 0 when every solve returned 0.
+ * Problems must be distinct handles. */
+int bdg_solve_batch(bdg_t **problems, int n, int concurrency, int graphs, int *rcs_out, double *seconds_out);
+
+/* Free a problem's solver workspace and device scratch (results and the
+ * problem's set-up stay; the next bdg_solve reallocates them). */
+void bdg_release_device_memory(bdg_t *bdg);
+
 #ifdef __cplusplus
 }
 #endif

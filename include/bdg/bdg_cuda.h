@@ -81,6 +81,25 @@ int bdgd_set_dipolar(bdgd_ctx *ctx, const double *vdd, double g_ddi, int enabled
 int bdgd_apply(bdgd_ctx *ctx, int op, int prec, const void *d_x, uint64_t ldx,
                void *d_y, uint64_t ldy, uint64_t ncol);
 
+/* Replay operator applies as CUDA graphs (on = 1): the first apply of a
+ * given (operator, precision, pointers, leading dimensions, columns) runs
+ * directly, the second is captured, later ones launch the graph.  Every
+ * field setter invalidates the recorded graphs.  Off by default; the
+ * environment variable BDG_GRAPHS=1 turns it on for new contexts.  (No
+ * counterpart in the reference, which applies one column per FFTW call.) */
+int bdgd_set_graphs(bdgd_ctx *ctx, int on);
+
+/* Free the context's apply scratch (spectra, staging, Gram partials) and its
+ * recorded graphs; they are reallocated on the next use. */
+int bdgd_trim(bdgd_ctx *ctx);
+
+/* FFT pass family the autotuner chose for (op, prec) on this context: 0 not
+ * tuned yet, 1 register-resident line transforms, 2 compile-time
+ * shared-memory stages; ms_out (2 floats, may be NULL) receives the timed
+ * milliseconds of both.  Tuning happens on the first apply of >= 4 columns
+ * unless BDG_FFT_PATH or BDG_GENERIC_FFT fixes the family. */
+int bdgd_fft_tuning(bdgd_ctx *ctx, int op, int prec, int *path_out, float *ms_out);
+
 /* Same as bdgd_apply on host memory (copies in, applies, copies out). */
 int bdgd_apply_host(bdgd_ctx *ctx, int op, const void *x, void *y, uint64_t ncol);
 
