@@ -580,7 +580,7 @@ static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, doubl
     }
   }
   g.segbase[g.ntiles] = sb;
-  int rc = bdgd_ensure((void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * (size_t)sb * GT * GT * es);
+  int rc = bdgd_ensure(c->stream, (void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * (size_t)sb * GT * GT * es);
   if (rc) return rc;
   g.part = c->gram_part;
   bdgd_count_launch();
@@ -690,7 +690,7 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
     g.t[i].part0 = off;
     off += (long long)nsplit * g.t[i].ka * g.t[i].kb * es;
   }
-  int rc = bdgd_ensure((void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
+  int rc = bdgd_ensure(c->stream, (void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
   if (rc) return rc;
   g.part = c->gram_part;
   // tasks with fewer rows than nsplit*chunk simply see empty splits (zeros)

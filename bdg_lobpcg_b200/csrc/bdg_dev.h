@@ -95,7 +95,7 @@ void bdgd_count_launch(void);
 // error helpers (defined in bdg_ops.cu)
 void bdgd_set_error(const char *fmt, ...);
 int bdgd_check(cudaError_t e, const char *what);
-int bdgd_ensure(void **ptr, size_t *have, size_t want);
+int bdgd_ensure(cudaStream_t st, void **ptr, size_t *have, size_t want);
 
 #define BDGD_CK(call)                                   \
   do {                                                  \

@@ -67,13 +67,15 @@ extern "C" int bdgd_device_count(void) {
   return n;
 }
 
-int bdgd_ensure(void **ptr, size_t *have, size_t want) {
+// Grow a scratch buffer, stream-ordered on st (no device-wide sync, so
+// solves on other streams keep running).
+int bdgd_ensure(cudaStream_t st, void **ptr, size_t *have, size_t want) {
   if (*have >= want && *ptr) return BDGD_OK;
-  if (*ptr) cudaFree(*ptr);
+  if (*ptr) BDGD_CK(cudaFreeAsync(*ptr, st));
   *ptr = nullptr;
   *have = 0;
   if (want == 0) return BDGD_OK;
-  BDGD_CK(cudaMalloc(ptr, want));
+  BDGD_CK(cudaMallocAsync(ptr, want, st));
   *have = want;
   return BDGD_OK;
 }
@@ -730,6 +732,19 @@ extern "C" int bdgd_create(bdgd_ctx **out, uint64_t dim, const uint64_t *N, cons
     bdgd_set_error("bdgd_create: no CUDA device");
     return BDGD_ERR_CUDA;
   }
+  {
+    // keep freed stream-ordered scratch in the device pool for reuse
+    static int pool_done[64];
+    if (c->device >= 0 && c->device < 64 && !pool_done[c->device]) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+      }
+      cudaGetLastError();
+      pool_done[c->device] = 1;
+    }
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     free(c);
@@ -804,9 +819,13 @@ extern "C" void bdgd_destroy(bdgd_ctx **pc) {
     cudaFree(c->d_kx2[d]);
   }
   void *bufs[] = {c->ltK64, c->ltM64, c->pK64, c->pM64, c->ltK32, c->ltM32, c->pK32, c->pM32,
-                  c->wf64,  c->wf32,  c->vdd,  c->spec, c->io,    c->gram_part, c->ptab};
+                  c->wf64,  c->wf32,  c->vdd,  c->ptab};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  void *sbufs[] = {c->spec, c->io, c->gram_part};  // stream-ordered (bdgd_ensure)
+  for (void *b : sbufs)
+    if (b) cudaFreeAsync(b, c->stream);
+  if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   free(c);
   *pc = nullptr;
@@ -1064,7 +1083,7 @@ static int run_program(bdgd_ctx *c, const Prog &p, const void *x, long long ldx,
   }
   if (only_fwd || only_bwd) chunk = ncol;  // raw transforms use the whole scratch as I/O
   void *spec_before = c->spec;
-  int rc = bdgd_ensure(&c->spec, &c->spec_bytes, per_col * (size_t)chunk);
+  int rc = bdgd_ensure(c->stream, &c->spec, &c->spec_bytes, per_col * (size_t)chunk);
   if (rc) return rc;
   if (c->spec != spec_before) c->version++;  // captured graphs hold the old scratch
   C *spec = (C *)c->spec;
@@ -1221,7 +1240,7 @@ extern "C" int bdgd_trim(bdgd_ctx *c) {
   void **bufs[] = {&c->spec, &c->io, (void **)&c->gram_part};
   size_t *sizes[] = {&c->spec_bytes, &c->io_bytes, &c->gram_part_bytes};
   for (int i = 0; i < 3; ++i) {
-    if (*bufs[i]) cudaFree(*bufs[i]);
+    if (*bufs[i]) BDGD_CK(cudaFreeAsync(*bufs[i], c->stream));
     *bufs[i] = nullptr;
     *sizes[i] = 0;
   }
@@ -1401,7 +1420,7 @@ extern "C" int bdgd_apply_host(bdgd_ctx *c, int op, const void *x, void *y, uint
   const int two = (op == BDGD_OP_LREP || op == BDGD_OP_TLREP || op == BDGD_OP_SWAP) ? 2 : 1;
   const size_t esz = c->cplx ? 16 : 8;
   const size_t colb = (size_t)c->S * two * esz;
-  int rc = bdgd_ensure(&c->io, &c->io_bytes, 2 * colb * ncol);
+  int rc = bdgd_ensure(c->stream, &c->io, &c->io_bytes, 2 * colb * ncol);
   if (rc) return rc;
   char *dx = (char *)c->io;
   char *dy = dx + colb * ncol;
@@ -1420,7 +1439,7 @@ extern "C" int bdgd_dipolar_meanfield(bdgd_ctx *c, double *phi_out) {
   }
   Prog p = make_prog(100, 0);
   const size_t esz = c->cplx ? 16 : 8;
-  int rc = bdgd_ensure(&c->io, &c->io_bytes, 2 * esz * c->S);
+  int rc = bdgd_ensure(c->stream, &c->io, &c->io_bytes, 2 * esz * c->S);
   if (rc) return rc;
   char *dx = (char *)c->io;
   char *dy = dx + esz * c->S;
@@ -1444,9 +1463,9 @@ extern "C" int bdgd_fft_host(bdgd_ctx *c, int forward, const void *in, void *out
   const size_t esz = c->cplx ? 16 : 8;
   const size_t rb = esz * (size_t)c->S * ncol;
   const size_t kb = 16 * (size_t)c->H * ncol;
-  int rc = bdgd_ensure(&c->io, &c->io_bytes, rb);
+  int rc = bdgd_ensure(c->stream, &c->io, &c->io_bytes, rb);
   if (rc) return rc;
-  rc = bdgd_ensure(&c->spec, &c->spec_bytes, kb);
+  rc = bdgd_ensure(c->stream, &c->spec, &c->spec_bytes, kb);
   if (rc) return rc;
   if (forward) {
     BDGD_CK(cudaMemcpyAsync(c->io, in, rb, cudaMemcpyHostToDevice, c->stream));

@@ -78,17 +78,26 @@ typedef struct {
   uint64_t cap_S, cap_m, cap_nev;
   int cap_cplx, cap_prec;
   cudaEvent_t ev[12];
+  cudaStream_t st; /* the context stream: workspace memory is stream-ordered on it */
 } ws_t;
+
+/* Stream-ordered device memory (cudaMallocAsync / cudaFreeAsync on the
+ * context stream): a solve that allocates or releases its workspace does not
+ * synchronise the device, so concurrent solves on other streams keep
+ * running (bdg_solve_batch). */
+static void dfree(ws_t *w, void *p) {
+  if (p) cudaFreeAsync(p, w->st);
+}
 
 static void ws_free(ws_t *w) {
   if (!w) return;
   for (int i = 0; i < NB_COUNT; i++)
-    if (w->blk[i]) cudaFree(w->blk[i]);
+    if (w->blk[i]) dfree(w, w->blk[i]);
   void *bufs[] = {w->TR, w->gout, w->Gs, w->Gb, w->Ga, w->Z, w->Ya, w->Hh, w->V, w->C, w->Cs, w->T1s, w->T2s,
                   w->dsc, w->wG, w->wA, w->wH, w->wtmp, w->lam_d, w->work, w->norms, w->C32, w->colmap,
                   w->actcols, w->defl, w->swork, w->info};
   for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; i++)
-    if (bufs[i]) cudaFree(bufs[i]);
+    if (bufs[i]) dfree(w, bufs[i]);
   if (w->blas) cublasDestroy(w->blas);
   if (w->sol) cusolverDnDestroy(w->sol);
   for (int i = 0; i < 12; i++)
@@ -146,8 +155,8 @@ const void *bdg_solver_block(const bdg_t *bdg) { return bdg->block; }
     if (_r) return _r;      \
   } while (0)
 
-static int dmalloc(void **p, size_t bytes) {
-  CUDA_TRY(cudaMalloc(p, bytes ? bytes : 16));
+static int dmalloc(ws_t *w, void **p, size_t bytes) {
+  CUDA_TRY(cudaMallocAsync(p, bytes ? bytes : 16, w->st));
   return 0;
 }
 
@@ -160,6 +169,7 @@ static int ws_setup(ws_t *w, bdgd_ctx *dev, uint64_t S, uint64_t m, uint64_t nev
     return 0;
   }
   ws_free(w);
+  w->st = stream_of(dev);
   w->S = S;
   w->n = 2 * S;
   w->m = m;
@@ -168,21 +178,21 @@ static int ws_setup(ws_t *w, bdgd_ctx *dev, uint64_t S, uint64_t m, uint64_t nev
   w->prec = prec;
   w->esz = (size_t)(prec == BDGD_F32 ? 4 : 8) * (cplx ? 2 : 1);
   w->K = (int)(3 * m);
-  for (int i = 0; i < NB_COUNT; i++) TRY(dmalloc(&w->blk[i], w->n * m * w->esz));
-  TRY(dmalloc(&w->TR, S * nev * w->esz));
+  for (int i = 0; i < NB_COUNT; i++) TRY(dmalloc(w, &w->blk[i], w->n * m * w->esz));
+  TRY(dmalloc(w, &w->TR, S * nev * w->esz));
   const size_t es = cplx ? 2 : 1;
   const size_t kk = (size_t)w->K * w->K * es * sizeof(double);
-  TRY(dmalloc((void **)&w->gout, 3 * kk));
+  TRY(dmalloc(w, (void **)&w->gout, 3 * kk));
   double **sm[] = {&w->Gs, &w->Gb, &w->Ga, &w->Z, &w->Ya, &w->Hh, &w->V, &w->C, &w->Cs, &w->T1s, &w->T2s};
-  for (size_t i = 0; i < sizeof sm / sizeof sm[0]; i++) TRY(dmalloc((void **)sm[i], kk));
-  TRY(dmalloc((void **)&w->C32, kk));
+  for (size_t i = 0; i < sizeof sm / sizeof sm[0]; i++) TRY(dmalloc(w, (void **)sm[i], kk));
+  TRY(dmalloc(w, (void **)&w->C32, kk));
   double **vec[] = {&w->dsc, &w->wG, &w->wA, &w->wH, &w->wtmp, &w->lam_d};
-  for (size_t i = 0; i < sizeof vec / sizeof vec[0]; i++) TRY(dmalloc((void **)vec[i], (size_t)w->K * sizeof(double)));
-  TRY(dmalloc((void **)&w->work, 2 * 64 * (size_t)w->K * sizeof(double)));
-  TRY(dmalloc((void **)&w->norms, 4 * (size_t)w->K * sizeof(double)));
-  TRY(dmalloc((void **)&w->colmap, (size_t)w->K * sizeof(int)));
-  TRY(dmalloc((void **)&w->actcols, (size_t)w->K * sizeof(int)));
-  TRY(dmalloc((void **)&w->info, sizeof(int)));
+  for (size_t i = 0; i < sizeof vec / sizeof vec[0]; i++) TRY(dmalloc(w, (void **)vec[i], (size_t)w->K * sizeof(double)));
+  TRY(dmalloc(w, (void **)&w->work, 2 * 64 * (size_t)w->K * sizeof(double)));
+  TRY(dmalloc(w, (void **)&w->norms, 4 * (size_t)w->K * sizeof(double)));
+  TRY(dmalloc(w, (void **)&w->colmap, (size_t)w->K * sizeof(int)));
+  TRY(dmalloc(w, (void **)&w->actcols, (size_t)w->K * sizeof(int)));
+  TRY(dmalloc(w, (void **)&w->info, sizeof(int)));
   BLAS_TRY(cublasCreate(&w->blas));
   BLAS_TRY(cublasSetStream(w->blas, stream_of(dev)));
   SOL_TRY(cusolverDnCreate(&w->sol));
@@ -192,12 +202,12 @@ static int ws_setup(ws_t *w, bdgd_ctx *dev, uint64_t S, uint64_t m, uint64_t nev
     SOL_TRY(cusolverDnZheevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, w->K,
                                         (cuDoubleComplex *)w->Gs, w->K, w->wG, &lw));
     w->lwork = lw;
-    TRY(dmalloc(&w->swork, (size_t)lw * sizeof(cuDoubleComplex)));
+    TRY(dmalloc(w, &w->swork, (size_t)lw * sizeof(cuDoubleComplex)));
   } else {
     SOL_TRY(cusolverDnDsyevd_bufferSize(w->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, w->K, w->Gs, w->K,
                                         w->wG, &lw));
     w->lwork = lw;
-    TRY(dmalloc(&w->swork, (size_t)lw * sizeof(double)));
+    TRY(dmalloc(w, &w->swork, (size_t)lw * sizeof(double)));
   }
   for (int i = 0; i < 12; i++) CUDA_TRY(cudaEventCreate(&w->ev[i]));
   w->cap_S = S;
@@ -448,7 +458,7 @@ static int deflate_block(ws_t *w, bdgd_ctx *dev, void *V, int q) {
 static int goldstone_setup(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int prec) {
   const int S = (int)w->S;
   double *x, *r, *p, *q, *psi;
-  TRY(dmalloc((void **)&x, 5 * (size_t)S * sizeof(double)));
+  TRY(dmalloc(w, (void **)&x, 5 * (size_t)S * sizeof(double)));
   r = x + S;
   p = r + S;
   q = p + S;
@@ -480,9 +490,9 @@ static int goldstone_setup(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int 
   double wpsi = 0;
   BLAS_TRY(cublasDdot(w->blas, S, x, 1, psi, 1, &wpsi));
   w->wpsi = wpsi;
-  if (w->defl) cudaFree(w->defl);
+  if (w->defl) dfree(w, w->defl);
   w->defl = NULL;
-  TRY(dmalloc((void **)&w->defl, 2 * (size_t)S * sizeof(double)));
+  TRY(dmalloc(w, (void **)&w->defl, 2 * (size_t)S * sizeof(double)));
   if (prec == BDGD_F32) {
     DEV_TRY(bdgd_convert(dev, 1, psi, w->defl, (uint64_t)S));
     DEV_TRY(bdgd_convert(dev, 1, x, (float *)w->defl + S, (uint64_t)S));
@@ -491,7 +501,7 @@ static int goldstone_setup(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int 
     CUDA_TRY(cudaMemcpyAsync(w->defl + S, x, (size_t)S * sizeof(double), cudaMemcpyDeviceToDevice, st));
   }
   CUDA_TRY(cudaStreamSynchronize(st));
-  cudaFree(x);
+  dfree(w, x);
   w->deflate = 1;
   return 0;
 }
@@ -854,11 +864,11 @@ static int solve_gpu(bdg_t *bdg) {
   bdg_fill_initial_block(bdg, X0);
   if (mixed) {
     void *tmp = NULL;
-    if ((rc = dmalloc(&tmp, n * m * hesz))) return rc;
+    if ((rc = dmalloc(w, &tmp, n * m * hesz))) return rc;
     CUDA_TRY(cudaMemcpyAsync(tmp, X0, n * m * hesz, cudaMemcpyHostToDevice, st));
     DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
     CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(tmp);
+    dfree(w, tmp);
   } else {
     CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, n * m * hesz, cudaMemcpyHostToDevice, st));
   }
