@@ -55,6 +55,7 @@ class SolveStats(C.Structure):
         ("ms_gram", C.c_double), ("ms_small_dense", C.c_double), ("ms_update", C.c_double),
         ("cols_apply_A", C.c_uint64), ("cols_apply_T", C.c_uint64),
         ("max_residual", C.c_double), ("max_true_residual", C.c_double), ("status", C.c_int),
+        ("seconds_setup", C.c_double), ("seconds_output", C.c_double),
     ]
 
     def as_dict(self):

@@ -64,6 +64,9 @@ void bdg_reset(bdg_t *bdg) {
   safe_free((void **)&bdg->eigvals);
   safe_free(&bdg->modes_u);
   safe_free(&bdg->modes_v);
+  safe_free(&bdg->block);
+  bdg->modes_bytes = 0;
+  bdg->block_ws = -1;
   bdg->converged = 0;
   bdg->state = BDG_HAS_SYSTEM;
 }

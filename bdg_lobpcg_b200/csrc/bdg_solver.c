@@ -79,6 +79,10 @@ typedef struct {
   int cap_cplx, cap_prec;
   cudaEvent_t ev[12];
   cudaStream_t st; /* the context stream: workspace memory is stream-ordered on it */
+  void *pin[2];    /* pinned host staging for block transfers */
+  cudaEvent_t pin_ev[2];
+  void *hX0;       /* pinned host initial block (kept across solves) */
+  size_t hX0_bytes;
 } ws_t;
 
 /* Stream-ordered device memory (cudaMallocAsync / cudaFreeAsync on the
@@ -102,7 +106,68 @@ static void ws_free(ws_t *w) {
   if (w->sol) cusolverDnDestroy(w->sol);
   for (int i = 0; i < 12; i++)
     if (w->ev[i]) cudaEventDestroy(w->ev[i]);
+  for (int i = 0; i < 2; i++) {
+    if (w->pin_ev[i]) cudaEventSynchronize(w->pin_ev[i]);
+    if (w->pin[i]) cudaFreeHost(w->pin[i]);
+    if (w->pin_ev[i]) cudaEventDestroy(w->pin_ev[i]);
+  }
+  if (w->hX0) {
+    if (w->st) cudaStreamSynchronize(w->st);
+    cudaFreeHost(w->hX0);
+  }
   memset(w, 0, sizeof *w);
+}
+
+/* Host <-> device copy of pageable user memory through two pinned staging
+ * buffers: the DMA of one chunk overlaps the host memcpy of the next
+ * (pageable copies run at a fraction of the pinned rate). */
+#define PIN_BYTES ((size_t)32 << 20)
+static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2d) {
+  for (int i = 0; i < 2; i++) {
+    if (!w->pin[i] && cudaMallocHost(&w->pin[i], PIN_BYTES) != cudaSuccess) {
+      cudaGetLastError();
+      w->pin[i] = NULL;
+    }
+    if (!w->pin_ev[i]) cudaEventCreateWithFlags(&w->pin_ev[i], cudaEventDisableTiming);
+  }
+  if (!w->pin[0] || !w->pin[1]) { /* no pinned memory: plain copy */
+    if (cudaMemcpyAsync(dst, src, bytes, h2d ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, w->st) !=
+        cudaSuccess)
+      return -3;
+    return cudaStreamSynchronize(w->st) == cudaSuccess ? 0 : -3;
+  }
+  const size_t nch = (bytes + PIN_BYTES - 1) / PIN_BYTES;
+  for (size_t i = 0; i < nch; i++) {
+    const int b = (int)(i & 1);
+    const size_t off = i * PIN_BYTES, len = (bytes - off) < PIN_BYTES ? (bytes - off) : PIN_BYTES;
+    if (h2d) {
+      if (i >= 2 && cudaEventSynchronize(w->pin_ev[b]) != cudaSuccess) return -3;
+      memcpy(w->pin[b], (const char *)src + off, len);
+      if (cudaMemcpyAsync((char *)dst + off, w->pin[b], len, cudaMemcpyHostToDevice, w->st) != cudaSuccess) return -3;
+      cudaEventRecord(w->pin_ev[b], w->st);
+    } else {
+      if (cudaMemcpyAsync(w->pin[b], (const char *)src + off, len, cudaMemcpyDeviceToHost, w->st) != cudaSuccess)
+        return -3;
+      cudaEventRecord(w->pin_ev[b], w->st);
+      if (i >= 1) { /* drain the previous chunk while this one is in flight */
+        const int pb = b ^ 1;
+        const size_t poff = off - PIN_BYTES;
+        if (cudaEventSynchronize(w->pin_ev[pb]) != cudaSuccess) return -3;
+        memcpy((char *)dst + poff, w->pin[pb], PIN_BYTES);
+      }
+    }
+  }
+  if (!h2d && nch > 0) {
+    const int lb = (int)((nch - 1) & 1);
+    const size_t loff = (nch - 1) * PIN_BYTES;
+    if (cudaEventSynchronize(w->pin_ev[lb]) != cudaSuccess) return -3;
+    memcpy((char *)dst + loff, w->pin[lb], bytes - loff);
+  }
+  if (h2d && nch > 0) { /* the staging buffers are reused: wait for the last copies */
+    for (int i = 0; i < 2; i++)
+      if (cudaEventSynchronize(w->pin_ev[i]) != cudaSuccess) return -3;
+  }
+  return 0;
 }
 
 void bdg_solver_release(bdg_t *bdg) {
@@ -115,7 +180,32 @@ void bdg_solver_release(bdg_t *bdg) {
   safe_free(&bdg->block);
 }
 
-const void *bdg_solver_block(const bdg_t *bdg) { return bdg->block; }
+static int dmalloc(ws_t *w, void **p, size_t bytes);
+static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2d);
+
+const void *bdg_solver_block(const bdg_t *cbdg) {
+  bdg_t *bdg = (bdg_t *)cbdg;
+  if (bdg->block || bdg->block_ws < 0 || !bdg->solver_ws) return bdg->block;
+  ws_t *w = &((ws_t *)bdg->solver_ws)[bdg->block_ws];
+  if (!w->blk[NB_X]) return NULL;
+  const size_t hesz = w->cplx ? sizeof(c64) : sizeof(f64);
+  const size_t eb = w->prec == BDGD_F32 ? hesz / 2 : hesz;
+  void *dev_blk = w->blk[NB_X];
+  void *tmp = NULL;
+  if (w->prec == BDGD_F32) { /* widen the FP32 block on the device */
+    if (dmalloc(w, &tmp, w->n * w->m * hesz)) return NULL;
+    if (bdgd_convert(bdg->ctx->dev, 0, dev_blk, tmp, w->n * w->m * (w->cplx ? 2 : 1))) {
+      dfree(w, tmp);
+      return NULL;
+    }
+    dev_blk = tmp;
+  }
+  (void)eb;
+  bdg->block = xmalloc(w->n * w->m * hesz);
+  if (staged_copy(w, bdg->block, dev_blk, w->n * w->m * hesz, 0)) safe_free(&bdg->block);
+  if (tmp) dfree(w, tmp);
+  return bdg->block;
+}
 
 #define CUDA_TRY(x)                                                              \
   do {                                                                           \
@@ -158,6 +248,61 @@ const void *bdg_solver_block(const bdg_t *bdg) { return bdg->block; }
 static int dmalloc(ws_t *w, void **p, size_t bytes) {
   CUDA_TRY(cudaMallocAsync(p, bytes ? bytes : 16, w->st));
   return 0;
+}
+
+/* Device-to-host copy of nseg segments (each <= PIN_BYTES) through the two
+ * pinned staging buffers, the memcpy of one overlapping the DMA of the next. */
+static int staged_d2h_segments(ws_t *w, int nseg, void *const *dst, const void *const *src, const size_t *len) {
+  if (!w->pin[0] || !w->pin[1]) {
+    for (int i = 0; i < nseg; i++)
+      if (cudaMemcpyAsync(dst[i], src[i], len[i], cudaMemcpyDeviceToHost, w->st) != cudaSuccess) return -3;
+    return cudaStreamSynchronize(w->st) == cudaSuccess ? 0 : -3;
+  }
+  for (int i = 0; i < nseg; i++) {
+    const int b = i & 1;
+    if (cudaMemcpyAsync(w->pin[b], src[i], len[i], cudaMemcpyDeviceToHost, w->st) != cudaSuccess) return -3;
+    cudaEventRecord(w->pin_ev[b], w->st);
+    if (i >= 1) {
+      if (cudaEventSynchronize(w->pin_ev[b ^ 1]) != cudaSuccess) return -3;
+      memcpy(dst[i - 1], w->pin[b ^ 1], len[i - 1]);
+    }
+  }
+  if (nseg > 0) {
+    const int lb = (nseg - 1) & 1;
+    if (cudaEventSynchronize(w->pin_ev[lb]) != cudaSuccess) return -3;
+    memcpy(dst[nseg - 1], w->pin[lb], len[nseg - 1]);
+  }
+  return 0;
+}
+
+/* Download columns [0, ncol) of a device block (leading dim n elements of
+ * esz bytes) as their u halves into mu and v halves into mv (S x ncol each). */
+static int download_modes(ws_t *w, const void *blk, uint64_t n, uint64_t S, uint64_t ncol, size_t esz, char *mu,
+                          char *mv) {
+  const size_t half = S * esz;
+  const size_t per = half < PIN_BYTES ? half : PIN_BYTES;
+  const size_t pieces = (half + per - 1) / per;
+  const size_t nseg = 2 * ncol * pieces;
+  void **dst = (void **)malloc(nseg * sizeof(void *));
+  const void **src = (const void **)malloc(nseg * sizeof(void *));
+  size_t *len = (size_t *)malloc(nseg * sizeof(size_t));
+  size_t k = 0;
+  for (uint64_t j = 0; j < ncol; j++)
+    for (int h = 0; h < 2; h++)
+      for (size_t q = 0; q < pieces; q++) {
+        const size_t off = q * per, l = (half - off) < per ? (half - off) : per;
+        dst[k] = (h ? mv : mu) + j * half + off;
+        src[k] = (const char *)blk + (j * n + (uint64_t)h * S) * esz + off;
+        len[k] = l;
+        k++;
+      }
+  /* make sure the staging buffers exist */
+  int rc = staged_copy(w, dst[0], src[0], 0, 0);
+  if (!rc) rc = staged_d2h_segments(w, (int)nseg, dst, src, len);
+  free(dst);
+  free(src);
+  free(len);
+  return rc;
 }
 
 static cudaStream_t stream_of(bdgd_ctx *dev) { return (cudaStream_t)bdgd_stream(dev); }
@@ -840,8 +985,7 @@ static int solve_gpu(bdg_t *bdg) {
     return -7;
   }
   safe_free((void **)&bdg->eigvals);
-  safe_free(&bdg->modes_u);
-  safe_free(&bdg->modes_v);
+  bdg->block_ws = -1;
   int rc = bdg_ctx_sync_device(ctx, BDGD_OP_LREP);
   if (!rc) rc = bdg_ctx_sync_device(ctx, BDGD_OP_TLREP);
   if (rc) {
@@ -860,19 +1004,38 @@ static int solve_gpu(bdg_t *bdg) {
   if (deflate && (rc = goldstone_setup(w, dev, ctx, w->prec))) return rc;
   /* initial block: host fill, upload (converted for FP32) */
   const size_t hesz = cplx ? sizeof(c64) : sizeof(f64);
-  void *X0 = xcalloc(n * m, hesz);
+  const size_t xb = n * m * hesz;
+  if (w->hX0_bytes != xb) {
+    if (w->hX0) cudaFreeHost(w->hX0);
+    w->hX0 = NULL;
+    w->hX0_bytes = 0;
+    if (cudaMallocHost(&w->hX0, xb) != cudaSuccess) {
+      cudaGetLastError();
+      w->hX0 = NULL;
+    } else {
+      w->hX0_bytes = xb;
+    }
+  }
+  const int pinned = w->hX0 != NULL;
+  void *X0 = pinned ? w->hX0 : xmalloc(xb);
+  /* a custom init fills every entry; the other modes rely on a zeroed block */
+  if (bdg->init_mode != BDG_INIT_CUSTOM) memset(X0, 0, xb);
   bdg_fill_initial_block(bdg, X0);
   if (mixed) {
     void *tmp = NULL;
-    if ((rc = dmalloc(w, &tmp, n * m * hesz))) return rc;
-    CUDA_TRY(cudaMemcpyAsync(tmp, X0, n * m * hesz, cudaMemcpyHostToDevice, st));
+    if ((rc = dmalloc(w, &tmp, xb))) return rc;
+    if (pinned) CUDA_TRY(cudaMemcpyAsync(tmp, X0, xb, cudaMemcpyHostToDevice, st));
+    else TRY(staged_copy(w, tmp, X0, xb, 1));
     DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
     CUDA_TRY(cudaStreamSynchronize(st));
     dfree(w, tmp);
+  } else if (pinned) {
+    CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, xb, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
   } else {
-    CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, n * m * hesz, cudaMemcpyHostToDevice, st));
+    TRY(staged_copy(w, w->blk[NB_X], X0, xb, 1));
   }
-  free(X0);
+  if (!pinned) free(X0);
   const double anorm = anorm_estimate(ctx);
   double *lam = xcalloc(3 * m, sizeof(double));
   double *res = xcalloc(nev, sizeof(double));
@@ -882,6 +1045,7 @@ static int solve_gpu(bdg_t *bdg) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
+  const double t_loop = now_s();
   loop_opts_t o;
   memset(&o, 0, sizeof o);
   o.criterion = bdg->criterion;
@@ -914,6 +1078,7 @@ static int solve_gpu(bdg_t *bdg) {
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);
   bdg->stats.seconds_device = 1e-3 * ev_ms(e0, e1);
+  const double t_out = now_s();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   bdg->stats.iterations = iters + iters2;
@@ -938,20 +1103,31 @@ static int solve_gpu(bdg_t *bdg) {
   bdg->converged = (uint64_t)nconv;
   bdg->eigvals = xcalloc(nev, sizeof(f64));
   memcpy(bdg->eigvals, lam, nev * sizeof(f64));
-  safe_free(&bdg->block);
-  bdg->block = xcalloc(n * m, hesz);
-  CUDA_TRY(cudaMemcpyAsync(bdg->block, w->blk[NB_X], n * m * hesz, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  char *mu = xcalloc(S * nev, hesz), *mv = xcalloc(S * nev, hesz);
-  for (uint64_t j = 0; j < nev; j++) {
-    memcpy(mu + j * S * hesz, (char *)bdg->block + j * n * hesz, S * hesz);
-    memcpy(mv + j * S * hesz, (char *)bdg->block + (j * n + S) * hesz, S * hesz);
+  safe_free(&bdg->block); /* downloaded on demand by bdg_solver_block */
+  bdg->block_ws = (w == &wsp[0]) ? 0 : 1;
+  /* the nev wanted modes, into the previous solve's buffers when they fit */
+  const size_t mb = S * nev * hesz;
+  if (!bdg->modes_u || !bdg->modes_v || bdg->modes_bytes != mb) {
+    safe_free(&bdg->modes_u);
+    safe_free(&bdg->modes_v);
+    bdg->modes_u = xmalloc(mb);
+    bdg->modes_v = xmalloc(mb);
+    bdg->modes_bytes = mb;
   }
-  bdg->modes_u = mu;
-  bdg->modes_v = mv;
+  if (w->prec == BDGD_F64) {
+    TRY(download_modes(w, w->blk[NB_X], n, S, nev, hesz, (char *)bdg->modes_u, (char *)bdg->modes_v));
+  } else { /* an FP32 block (mixed solve without refinement): widen on the device first */
+    void *tmp = NULL;
+    TRY(dmalloc(w, &tmp, n * nev * hesz));
+    DEV_TRY(bdgd_convert(dev, 0, w->blk[NB_X], tmp, n * nev * (cplx ? 2 : 1)));
+    TRY(download_modes(w, tmp, n, S, nev, hesz, (char *)bdg->modes_u, (char *)bdg->modes_v));
+    dfree(w, tmp);
+  }
   free(lam);
   free(res);
   bdg->stats.seconds_total = now_s() - t0;
+  bdg->stats.seconds_setup = t_loop - t0;
+  bdg->stats.seconds_output = now_s() - t_out;
   return 0;
 }
 

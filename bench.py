@@ -282,7 +282,7 @@ def main():
     peak = peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
     n = 2 * size
     h2d = n * cfg["sizeSub"] * 8 + size * 8 * 4  # initial block + fields
-    d2h = n * cfg["sizeSub"] * 8 + 2 * size * cfg["nev"] * 8 + cfg["nev"] * 8
+    d2h = 2 * size * cfg["nev"] * 8 + cfg["nev"] * 8  # the nev modes (u and v halves) + eigenvalues
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
@@ -297,6 +297,8 @@ def main():
         "eigenvalues_head": [float(v) for v in ev[:6]],
         "stage_ms": {k: st[k] for k in ("ms_apply_A", "ms_apply_T", "ms_residual", "ms_gram", "ms_small_dense",
                                          "ms_update")},
+        "e2e_split_s": {"setup": st["seconds_setup"], "loop_device": st["seconds_device"],
+                        "output": st["seconds_output"], "bdg_solve_wall": st["seconds_total"]},
         "ground_state": {"seconds": t_gs, "itp_steps": itp_steps, "mu": mu, "stationarity": stationarity},
         "roofline": {"bound": "hbm", "kernel": "batched Lrep apply (5 FFT pass kernels)",
                      "achieved": a_gbs, "peak": peak, "unit": "GB/s",

@@ -47,6 +47,8 @@ typedef struct {
   double max_residual;     /* final convergence measure over the nev pairs */
   double max_true_residual;/* final ||KMv - w^2 v||/||v|| over the nev pairs */
   int status;              /* 0 ok, <0 CUDA / numerical failure */
+  double seconds_setup;    /* wall time before the loop: fields, workspace, deflation, X0 fill and upload */
+  double seconds_output;   /* wall time after the loop: final measures, block and modes download */
 } bdg_solve_stats_t;
 
 void bdg_set_precision(bdg_t *bdg, int precision);
@@ -64,7 +66,9 @@ void bdg_set_trap_grid(bdg_t *bdg, const double *V);
 /* bdg_set_local_interactions with U_K(|psi_i|^2) and U_M(|psi_i|^2) already
  * evaluated per grid point; same state rules and accumulation. */
 void bdg_set_local_interactions_grid(bdg_t *bdg, const double *uK, const double *uM);
-/* Full solver block after a solve: n x sizeSub column-major (host), or NULL. */
+/* Full solver block after a solve: n x sizeSub column-major (host), or NULL.
+ * Downloaded on the first call after a solve (the solve itself only brings
+ * back the nev wanted modes); NULL once the device workspace is released. */
 const void *bdg_solver_block(const bdg_t *bdg);
 
 /* Stationary real condensate on the GPU: split-step imaginary-time

@@ -160,6 +160,8 @@ struct bdg_t {
   int64_t learned_fallback; /* iteration of the last fallback, or -1 */
   double *harvest;          /* device buffer of residual columns, or NULL */
   uint64_t harvest_cap, harvest_n;
+  int block_ws;             /* workspace holding the last solve's block (0/1), or -1 */
+  size_t modes_bytes;       /* allocation size of modes_u / modes_v (reused across solves) */
 };
 
 /* ---- context lifecycle (reference src/bdg_internal.h:151-153) ------------ */
