@@ -140,6 +140,7 @@ def lib():
         "bdgd_apply": (i, [vp, i, i, vp, u64, vp, u64, u64]),
         "bdgd_apply_host": (i, [vp, i, vp, vp, u64]),
         "bdgd_gram": (i, [vp, i, i, u64, u64, vp, u64, vp, u64, vp]),
+        "bdgd_block_update": (i, [vp, i, i, u64, u64, i, vp]),
         "bdg_lp_create": (i, [C.POINTER(vp), _u64p, i, i, i]),
         "bdg_lp_free": (None, [C.POINTER(vp)]),
         "bdg_lp_nparams": (u64, [vp]),
@@ -527,6 +528,15 @@ class Problem:
 # ---------------------------------------------------------------------------
 # device context (block entry points on device pointers)
 # ---------------------------------------------------------------------------
+class _UpdateTerm(C.Structure):
+    _fields_ = [("s", C.c_void_p), ("c", C.c_void_p), ("k", C.c_int), ("ldc", C.c_int)]
+
+
+class _UpdateOut(C.Structure):
+    _fields_ = [("y", C.c_void_p), ("ncol", C.c_int), ("nterm", C.c_int), ("alpha", C.c_double),
+                ("beta", C.c_double), ("term", _UpdateTerm * 3)]
+
+
 class DeviceContext:
     """bdgd_ctx: batched operator applies on device memory (bdg_cuda.h)."""
 
@@ -600,6 +610,17 @@ class DeviceContext:
     def gram_ptr(self, prec, cplx, half, k, S_ptr, lds, AS_ptr, ldas, out_ptr):
         self.check(self._L.bdgd_gram(self._c, prec, 1 if cplx else 0, half, k, C.c_void_p(S_ptr), lds,
                                      C.c_void_p(AS_ptr), ldas, C.c_void_p(out_ptr)))
+
+    def block_update(self, prec, cplx, n, ld, outs):
+        """bdgd_block_update: outs = [(y_ptr, ncol, alpha, beta, [(s_ptr, k, c_ptr, ldc), ...]), ...].
+        Returns the library's status (BDGD_ERR_UNSUPPORTED = -3 launches nothing)."""
+        arr = (_UpdateOut * len(outs))()
+        for o, (y, ncol, alpha, beta, terms) in zip(arr, outs):
+            o.y, o.ncol, o.nterm, o.alpha, o.beta = y, ncol, len(terms), alpha, beta
+            for t, (sp, k, cp, ldc) in zip(o.term, terms):
+                t.s, t.k, t.c, t.ldc = sp, k, cp, ldc
+        return self._L.bdgd_block_update(self._c, prec, 1 if cplx else 0, n, ld, len(outs),
+                                         C.cast(arr, C.c_void_p))
 
     def synchronize(self):
         self.check(self._L.bdgd_synchronize(self._c))

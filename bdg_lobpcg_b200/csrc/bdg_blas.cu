@@ -1237,3 +1237,238 @@ extern "C" int bdgd_set_ritz_block(bdgd_ctx *c, double *Ga, double *Guv, int ldo
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Block update Y_o = alpha_o * sum_b S_ob C_ob + beta_o * Y_o (FP64, real).
+//
+// The basis updates of iLOBPCG (X <- [X, P, W] C_x, P <- [P, W] C_p and their
+// A-images, the projections P -= X (X^H X)^+ X^H P and W -= Q (...), the SVQB
+// rotations) are n x k by k x ncol products with n = 2 N^3 rows and k, ncol
+// at most a few hundred: the other half of the solver's FP64 work beside the
+// Gram.  One launch serves up to UMAXO outputs, each a sum of up to three
+// terms, so X, AX, P, AP of the update step come out of one pass.  Tiles: 64
+// rows x 64 output columns per 128-thread block (four warps of 32 x 32), the
+// contraction walked in 32-column stages through a two-stage cp.async
+// pipeline: the S stage as [32 columns][64 rows] (16-byte copies along the
+// contiguous rows), the small matrix C as [64 output columns][32] (8-byte
+// copies, it may have any leading dimension).  Products on the FP64 tensor
+// cores (mma.sync m8n8k4).  Consecutive blocks take the output column tiles
+// of one row tile, so S tiles shared by several outputs are read from L2.
+// ---------------------------------------------------------------------------
+#define UMAXO 4
+#define UMAXCT 16
+#define UKC 16   // contraction columns per stage
+#define USTG 4   // stages in the cp.async ring
+#define ULDM 68  // S stage row: 64 rows + 4 (the 16 fragment addresses of a half-warp fall in distinct banks)
+#define ULDK 20  // C stage row: UKC + 4
+
+struct UTerm {
+  const double *s;
+  const double *c;
+  int k, ldc;
+};
+struct UOut {
+  double *y;
+  int ncol, nterm;
+  double alpha, beta;
+  UTerm t[3];
+};
+struct UArgs {
+  UOut o[UMAXO];
+  long long n, ld;
+  int nct;
+  signed char ct_out[UMAXCT], ct_col[UMAXCT];
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+
+// stage j of term tm: S columns [UKC j, UKC j + UKC) of rows [r0, r0 + 64) as
+// sA[column][row], and the matching UKC rows of C for output columns
+// [c0, c0 + 64) as sB[output column][k]; out-of-range entries are zero-filled
+__device__ __forceinline__ void upd_stage(double *sA, double *sB, const UTerm &tm, int j, long long r0, long long n,
+                                          long long ld, int c0, int ncol) {
+  const int kc0 = UKC * j;
+  for (int q = threadIdx.x; q < UKC * 32; q += 128) {
+    const int col = q >> 5, ch = q & 31;
+    const long long row = r0 + 2 * ch;
+    long long nv = n - row;
+    nv = nv < 0 ? 0 : (nv > 2 ? 2 : nv);
+    const bool ok = (kc0 + col) < tm.k && nv > 0;
+    const double *src = ok ? tm.s + (long long)(kc0 + col) * ld + row : tm.s;
+    cp_async16(sA + col * ULDM + 2 * ch, src, ok ? (int)(nv * 8) : 0);
+  }
+  for (int q = threadIdx.x; q < 64 * UKC; q += 128) {
+    const int oc = q / UKC, kk = q % UKC;
+    const bool ok = (c0 + oc) < ncol && (kc0 + kk) < tm.k;
+    const double *src = ok ? tm.c + (long long)(c0 + oc) * tm.ldc + kc0 + kk : tm.c;
+    cp_async8(sB + oc * ULDK + kk, src, ok ? 8 : 0);
+  }
+}
+
+// stages of output column task ct (sum over its terms of ceil(k / UKC))
+__device__ __forceinline__ int upd_nst(const UArgs &u, int ct) {
+  const UOut &o = u.o[u.ct_out[ct]];
+  int n = 0;
+  for (int b = 0; b < o.nterm; ++b) n += (o.t[b].k + UKC - 1) / UKC;
+  return n;
+}
+
+// Persistent: block b takes row tiles b, b + grid, ... and, for each, the
+// column tasks 0..nct-1 in turn (their S tiles are shared through L2); all
+// stages run through one USTG-deep cp.async ring, so the loads of a tile's
+// first stages overlap the previous tile's last products and its stores.
+// With beta != 0 the accumulators start at (beta / alpha) Y, loaded together
+// at the start of the tile (exact for the solver's alpha = +-1, beta = 1).
+__global__ void __launch_bounds__(128, 3) k_block_update(UArgs u, long long nrt) {
+  extern __shared__ __align__(16) unsigned char usm[];
+  double *buf = (double *)usm;  // [USTG][A: UKC x ULDM | B: 64 x ULDK]
+  constexpr int STG = UKC * ULDM + 64 * ULDK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = warp & 1, wj = warp >> 1;
+  const int lr = lane & 3, lc = lane >> 2;
+  // load cursor: row tile lrt, column task lct, term lb, stage lj within the term
+  long long lrt = blockIdx.x;
+  int lct = 0, lb = 0, lj = 0;
+  auto issue = [&](int slot) {
+    // the next stage of the load cursor into ring slot `slot` (an empty group when done)
+    if (lrt < nrt) {
+      const UOut &o = u.o[u.ct_out[lct]];
+      double *dst = buf + slot * STG;
+      upd_stage(dst, dst + UKC * ULDM, o.t[lb], lj, lrt * 64, u.n, u.ld, 64 * u.ct_col[lct], o.ncol);
+      if (++lj == (o.t[lb].k + UKC - 1) / UKC) {
+        lj = 0;
+        if (++lb == o.nterm) {
+          lb = 0;
+          if (++lct == u.nct) lct = 0, lrt += gridDim.x;
+        }
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < USTG - 1; ++q) issue(q);
+  double acc[4][4][2];
+  int slot = 0;
+  for (long long rt = blockIdx.x; rt < nrt; rt += gridDim.x)
+    for (int ct = 0; ct < u.nct; ++ct) {
+      const long long r0 = rt * 64;
+      const UOut &o = u.o[u.ct_out[ct]];
+      const int c0 = 64 * u.ct_col[ct];
+      const int nst = upd_nst(u, ct);
+      const double alpha = o.alpha, beta = o.beta;
+      double *y = o.y;
+      if (beta != 0.0) {
+        const double sc = beta / alpha;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const long long row = r0 + wi * 32 + mi * 8 + lc;
+              const int col = c0 + wj * 32 + nj * 8 + 2 * lr + e;
+              acc[mi][nj][e] = (row < u.n && col < o.ncol) ? sc * __ldcs(y + (long long)col * u.ld + row) : 0.0;
+            }
+      } else {
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj) acc[mi][nj][0] = acc[mi][nj][1] = 0.0;
+      }
+      for (int s = 0; s < nst; ++s) {
+        cp_async_wait<USTG - 2>();
+        __syncthreads();  // stage `slot` visible to all; the slot refilled below is no longer read
+        issue((slot + USTG - 1) % USTG);
+        const double *sA = buf + slot * STG, *sB = sA + UKC * ULDM;
+#pragma unroll
+        for (int kk = 0; kk < UKC; kk += 4) {
+          double ar[4], br[4];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi) ar[mi] = sA[(kk + lr) * ULDM + wi * 32 + mi * 8 + lc];
+#pragma unroll
+          for (int nj = 0; nj < 4; ++nj) br[nj] = sB[(wj * 32 + nj * 8 + lc) * ULDK + kk + lr];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+        }
+        slot = slot == USTG - 1 ? 0 : slot + 1;
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const long long row = r0 + wi * 32 + mi * 8 + lc;
+            const int col = c0 + wj * 32 + nj * 8 + 2 * lr + e;
+            if (row < u.n && col < o.ncol) __stcs(y + (long long)col * u.ld + row, alpha * acc[mi][nj][e]);
+          }
+    }
+  cp_async_wait<0>();
+}
+
+// resident blocks of k_block_update on this device (queried once per device)
+static int upd_slots(size_t sm) {
+  static int cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (cache[dev] <= 0) {
+    int nb = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_block_update, 128, sm) != cudaSuccess || nb < 1) nb = 1;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+    cache[dev] = nb * nsm;
+  }
+  return cache[dev];
+}
+
+extern "C" int bdgd_block_update(bdgd_ctx *c, int prec, int cplx, uint64_t n, uint64_t ld, int nout,
+                                 const bdgd_update_out *outs) {
+  if (nout <= 0 || n == 0) return BDGD_OK;
+  if (prec != BDGD_F64 || cplx || nout > UMAXO || ld < n || (ld & 1)) return BDGD_ERR_UNSUPPORTED;
+  UArgs u;
+  memset(&u, 0, sizeof u);
+  u.n = (long long)n;
+  u.ld = (long long)ld;
+  int nct = 0;
+  for (int i = 0; i < nout; ++i) {
+    const bdgd_update_out &s = outs[i];
+    if (s.nterm < 0 || s.nterm > 3 || s.ncol < 0 || ((uintptr_t)s.y % 8)) return BDGD_ERR_UNSUPPORTED;
+    UOut &o = u.o[i];
+    o.y = (double *)s.y;
+    o.ncol = s.ncol;
+    o.nterm = 0;
+    o.alpha = s.alpha;
+    o.beta = s.beta;
+    for (int b = 0; b < s.nterm; ++b) {
+      if (s.term[b].k <= 0) continue;
+      if (((uintptr_t)s.term[b].s % 16) || s.term[b].ldc < s.term[b].k || ((uintptr_t)s.term[b].c % 8))
+        return BDGD_ERR_UNSUPPORTED;
+      UTerm &t = o.t[o.nterm++];
+      t.s = (const double *)s.term[b].s;
+      t.c = s.term[b].c;
+      t.k = s.term[b].k;
+      t.ldc = s.term[b].ldc;
+    }
+    for (int j = 0; o.nterm > 0 && j * 64 < s.ncol; ++j) {  // no terms: Y untouched
+      if (nct == UMAXCT) return BDGD_ERR_UNSUPPORTED;
+      u.ct_out[nct] = (signed char)i;
+      u.ct_col[nct] = (signed char)j;
+      nct++;
+    }
+  }
+  if (nct == 0) return BDGD_OK;
+  u.nct = nct;
+  const long long nrt = ((long long)n + 63) / 64;
+  const size_t sm = sizeof(double) * USTG * (UKC * ULDM + 64 * ULDK);
+  if (!bdgd_capturing) BDGD_CK(cudaFuncSetAttribute(k_block_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const long long nblk = nrt < upd_slots(sm) ? nrt : upd_slots(sm);
+  bdgd_count_launch();
+  k_block_update<<<(unsigned)nblk, 128, sm, c->stream>>>(u, nrt);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}

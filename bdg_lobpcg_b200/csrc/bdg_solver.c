@@ -475,6 +475,47 @@ static int bgemm(ws_t *w, bdgd_ctx *dev, const void *X, int k, const double *Cm,
   return 0;
 }
 
+/* Y_o = alpha_o sum_b S_ob C_ob + beta_o Y_o for nout outputs.  With `fused`
+ * (real FP64 blocks, BDG_UPDATE_BLAS unset): one launch of the fused FP64
+ * update kernel, which beats one cuBLAS GEMM per term when the outputs share
+ * several terms (the basis update: 27 against 24 TF/s at 128^3); the
+ * single-term projections stay on cuBLAS, faster there (23 against 16 TF/s
+ * at k = 64 with beta = 1). */
+static int upd_term(bdgd_update_out *o, const void *S, int k, const double *Cm, int ldc) {
+  if (k <= 0) return 0;
+  bdgd_update_term *t = &o->term[o->nterm++];
+  t->s = S;
+  t->k = k;
+  t->c = Cm;
+  t->ldc = ldc;
+  return 0;
+}
+
+static bdgd_update_out upd_out(void *Y, int ncol, double alpha, double beta) {
+  bdgd_update_out o;
+  memset(&o, 0, sizeof o);
+  o.y = Y;
+  o.ncol = ncol;
+  o.alpha = alpha;
+  o.beta = beta;
+  return o;
+}
+
+static int bupdate(ws_t *w, bdgd_ctx *dev, int fused, int nout, const bdgd_update_out *o) {
+  if (fused && !getenv("BDG_UPDATE_BLAS") && w->prec == BDGD_F64 && !w->cplx) {
+    const int rc = bdgd_block_update(dev, w->prec, w->cplx, w->n, w->n, nout, o);
+    if (rc != BDGD_ERR_UNSUPPORTED) {
+      DEV_TRY(rc);
+      return 0;
+    }
+  }
+  for (int i = 0; i < nout; ++i)
+    for (int b = 0; b < o[i].nterm; ++b)
+      TRY(bgemm(w, dev, o[i].term[b].s, o[i].term[b].k, o[i].term[b].c, o[i].term[b].ldc, o[i].ncol, o[i].alpha,
+                b == 0 ? o[i].beta : 1.0, o[i].y));
+  return 0;
+}
+
 /* ---- Gram launches ---------------------------------------------------------- */
 static bdgd_gram_task mk_task(ws_t *w, const void *a, const void *b, uint64_t rows, int ka, int kb, int out, int i0,
                               int j0, int sym, int mirror) {
@@ -862,14 +903,22 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
       t[1] = mk_task(w, B(NB_X), B(NB_P), w->n, m, p, 0, 0, m, 0, 0);
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 2, t, K, w->gout));
       TRY(gram_pinv_apply(w, dev, w->gout, m, K, w->gout + (size_t)m * K * es, p, drop, w->Cs));
-      TRY(bgemm(w, dev, B(NB_X), m, w->Cs, m, p, -1.0, 1.0, B(NB_P)));
-      TRY(bgemm(w, dev, B(NB_AX), m, w->Cs, m, p, -1.0, 1.0, B(NB_AP)));
+      {
+        bdgd_update_out o[2] = {upd_out(B(NB_P), p, -1.0, 1.0), upd_out(B(NB_AP), p, -1.0, 1.0)};
+        upd_term(&o[0], B(NB_X), m, w->Cs, m);
+        upd_term(&o[1], B(NB_AX), m, w->Cs, m);
+        TRY(bupdate(w, dev, 0, 2, o));
+      }
       t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 1, 0, 0, 1, 0);
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
       TRY(svqb(w, dev, w->gout + (size_t)K * K * es, p, K, drop, w->Cs, &pk));
       /* Cs holds Z_P (p x pk, leading dim p) */
-      TRY(bgemm(w, dev, B(NB_P), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T1)));
-      TRY(bgemm(w, dev, B(NB_AP), p, w->Cs, p, pk, 1.0, 0.0, B(NB_T2)));
+      {
+        bdgd_update_out o[2] = {upd_out(B(NB_T1), pk, 1.0, 0.0), upd_out(B(NB_T2), pk, 1.0, 0.0)};
+        upd_term(&o[0], B(NB_P), p, w->Cs, p);
+        upd_term(&o[1], B(NB_AP), p, w->Cs, p);
+        TRY(bupdate(w, dev, 0, 2, o));
+      }
       swapb(w, NB_P, NB_T1);
       swapb(w, NB_AP, NB_T2);
     }
@@ -888,14 +937,22 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, nt, t, K, w->gout));
       TRY(gram_pinv_apply(w, dev, w->gout, q, K, w->gout + (size_t)q * K * es, na, drop, w->Cs));
       /* Cs: q x na (leading dim q) */
-      TRY(bgemm(w, dev, B(NB_X), m, w->Cs, q, na, -1.0, 1.0, B(NB_WT)));
-      if (pk > 0) TRY(bgemm(w, dev, B(NB_P), pk, w->Cs + (size_t)m * es, q, na, -1.0, 1.0, B(NB_WT)));
+      {
+        bdgd_update_out o = upd_out(B(NB_WT), na, -1.0, 1.0);
+        upd_term(&o, B(NB_X), m, w->Cs, q);
+        upd_term(&o, B(NB_P), pk, w->Cs + (size_t)m * es, q);
+        TRY(bupdate(w, dev, 0, 1, &o));
+      }
       t[0] = mk_task(w, B(NB_WT), B(NB_WT), w->n, na, na, 1, 0, 0, 1, 0);
       DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
     }
     int wk = 0;
     TRY(svqb(w, dev, w->gout + (size_t)K * K * es, na, K, drop, w->Cs, &wk));
-    TRY(bgemm(w, dev, B(NB_WT), na, w->Cs, na, wk, 1.0, 0.0, B(NB_W)));
+    {
+      bdgd_update_out o = upd_out(B(NB_W), wk, 1.0, 0.0);
+      upd_term(&o, B(NB_WT), na, w->Cs, na);
+      TRY(bupdate(w, dev, 0, 1, &o));
+    }
     cudaEventRecord(w->ev[6], st);
     DEV_TRY(bdgd_apply(dev, BDGD_OP_LREP, w->prec, B(NB_W), w->n, B(NB_AW), w->n, (uint64_t)wk));
     cudaEventRecord(w->ev[7], st);
@@ -915,14 +972,14 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     cudaEventRecord(w->ev[9], st);
     /* X <- X Cx + P Cp + W Cw ; P <- P Cp + W Cw on the active columns */
     const double *Cx = w->C, *Cp = w->C + (size_t)m * es, *Cw = w->C + (size_t)(m + pk) * es;
-    TRY(bgemm(w, dev, B(NB_X), m, Cx, k, m, 1.0, 0.0, B(NB_XN)));
-    TRY(bgemm(w, dev, B(NB_AX), m, Cx, k, m, 1.0, 0.0, B(NB_AXN)));
-    if (pk > 0) {
-      TRY(bgemm(w, dev, B(NB_P), pk, Cp, k, m, 1.0, 1.0, B(NB_XN)));
-      TRY(bgemm(w, dev, B(NB_AP), pk, Cp, k, m, 1.0, 1.0, B(NB_AXN)));
-    }
-    TRY(bgemm(w, dev, B(NB_W), wk, Cw, k, m, 1.0, 1.0, B(NB_XN)));
-    TRY(bgemm(w, dev, B(NB_AW), wk, Cw, k, m, 1.0, 1.0, B(NB_AXN)));
+    bdgd_update_out uo[4] = {upd_out(B(NB_XN), m, 1.0, 0.0), upd_out(B(NB_AXN), m, 1.0, 0.0),
+                             upd_out(B(NB_PN), na, 1.0, 0.0), upd_out(B(NB_APN), na, 1.0, 0.0)};
+    upd_term(&uo[0], B(NB_X), m, Cx, k);
+    upd_term(&uo[0], B(NB_P), pk, Cp, k);
+    upd_term(&uo[0], B(NB_W), wk, Cw, k);
+    upd_term(&uo[1], B(NB_AX), m, Cx, k);
+    upd_term(&uo[1], B(NB_AP), pk, Cp, k);
+    upd_term(&uo[1], B(NB_AW), wk, Cw, k);
     /* C restricted to the active columns and to the [P, W] rows */
     CUDA_TRY(cudaMemcpyAsync(w->actcols, act, (size_t)na * sizeof(int), cudaMemcpyHostToDevice, st));
     DEV_TRY(bdgd_gather_cols(dev, w->C + (size_t)m * es, k, pk + wk, w->actcols, na, w->cplx, w->T2s, pk + wk));
@@ -931,15 +988,12 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
       CUDA_TRY(cudaMemcpyAsync(w->Cs, w->T2s, (size_t)(pk + wk) * na * es * sizeof(double),
                                cudaMemcpyDeviceToDevice, st));
     }
-    if (pk > 0) {
-      TRY(bgemm(w, dev, B(NB_P), pk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_PN)));
-      TRY(bgemm(w, dev, B(NB_AP), pk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_APN)));
-      TRY(bgemm(w, dev, B(NB_W), wk, w->Cs + (size_t)pk * es, pk + wk, na, 1.0, 1.0, B(NB_PN)));
-      TRY(bgemm(w, dev, B(NB_AW), wk, w->Cs + (size_t)pk * es, pk + wk, na, 1.0, 1.0, B(NB_APN)));
-    } else {
-      TRY(bgemm(w, dev, B(NB_W), wk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_PN)));
-      TRY(bgemm(w, dev, B(NB_AW), wk, w->Cs, pk + wk, na, 1.0, 0.0, B(NB_APN)));
-    }
+    /* X, AX, P, AP of the next iteration in one pass over the blocks */
+    upd_term(&uo[2], B(NB_P), pk, w->Cs, pk + wk);
+    upd_term(&uo[2], B(NB_W), wk, w->Cs + (size_t)pk * es, pk + wk);
+    upd_term(&uo[3], B(NB_AP), pk, w->Cs, pk + wk);
+    upd_term(&uo[3], B(NB_AW), wk, w->Cs + (size_t)pk * es, pk + wk);
+    TRY(bupdate(w, dev, 1, 4, uo));
     swapb(w, NB_X, NB_XN);
     swapb(w, NB_AX, NB_AXN);
     swapb(w, NB_P, NB_PN);

@@ -3,6 +3,7 @@
     python -m bdg_lobpcg_b200.profile_ops [--grid 128] [--ncol 8] [--prec 0|1] [--reps 3]
                                           [--complex] [--time] [--paths reg,ct]
     python -m bdg_lobpcg_b200.profile_ops --gram 192 [--grid 128] [--prec 0|1] [--reps 5]
+    python -m bdg_lobpcg_b200.profile_ops --update 64 [--grid 128] [--reps 5]
 
 Random fields and columns on a grid^3 dipolar context.  Without --time it
 applies LREP and TLREP `reps` times each (after one warm-up apply), then one
@@ -20,6 +21,12 @@ on 2*grid^3 rows) and, for reference, cuBLAS FP64 through torch on the same
 contraction (S S^T and S AS^T of the K x n blocks) and on a square 8192^3
 FP64 GEMM, and prints the FLOP rates.  The library counts a symmetric block
 at tile granularity (64 x 64 tiles on and above the diagonal).
+
+With --update M it times the iLOBPCG basis update of one iteration on
+2*grid^3 rows with M columns per block: X' = [X P W] C_x and
+P' = [P W] C_p with their A-images (four outputs, one launch of
+bdgd_block_update), against the same products as four cuBLAS FP64 GEMMs
+through torch, and prints the FLOP rates.
 """
 import argparse
 import json
@@ -51,11 +58,14 @@ def main():
     ap.add_argument("--time", action="store_true")
     ap.add_argument("--paths", default="reg,ct")
     ap.add_argument("--gram", type=int, default=0)
+    ap.add_argument("--update", type=int, default=0)
     a = ap.parse_args()
     import torch
 
     if a.gram:
         return gram_main(a)
+    if a.update:
+        return update_main(a)
 
     import bdg_lobpcg_b200 as B
 
@@ -154,6 +164,79 @@ def gram_main(a):
     M = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
     ms3 = _time(lambda: torch.mm(M, M), cur, a.reps)
     print(json.dumps({"what": "cublas_fp64_square_8192", "ms": ms3, "tflops": 2.0 * 8192 ** 3 / ms3 / 1e9}))
+    return 0
+
+
+def update_main(a):
+    import torch
+
+    import bdg_lobpcg_b200 as B
+
+    m, n = a.update, 2 * a.grid ** 3
+    dc = B.DeviceContext(3, [a.grid] * 3, [24.0] * 3, False)
+    blk = {nm: torch.randn(m, n, dtype=torch.float64, device="cuda") for nm in ("X", "P", "W", "AX", "AP", "AW")}
+    out = {nm: torch.empty(m, n, dtype=torch.float64, device="cuda") for nm in ("XN", "AXN", "PN", "APN")}
+    Cx = torch.randn(m, 3 * m, dtype=torch.float64, device="cuda")  # (3m x m) column-major
+    Cp = torch.randn(m, 2 * m, dtype=torch.float64, device="cuda")  # (2m x m) column-major
+    stream = torch.cuda.ExternalStream(dc.stream)
+    e8 = 8
+
+    def terms(names, Cm, k):
+        return [(blk[nm].data_ptr(), m, Cm.data_ptr() + i * m * e8, k) for i, nm in enumerate(names)]
+
+    outs = [(out["XN"].data_ptr(), m, 1.0, 0.0, terms(("X", "P", "W"), Cx, 3 * m)),
+            (out["AXN"].data_ptr(), m, 1.0, 0.0, terms(("AX", "AP", "AW"), Cx, 3 * m)),
+            (out["PN"].data_ptr(), m, 1.0, 0.0, terms(("P", "W"), Cp, 2 * m)),
+            (out["APN"].data_ptr(), m, 1.0, 0.0, terms(("AP", "AW"), Cp, 2 * m))]
+
+    def lib():
+        rc = dc.block_update(0, False, n, n, outs)
+        if rc:
+            raise RuntimeError(f"bdgd_block_update: {rc}")
+
+    flops = 2.0 * n * m * (3 * m * 2 + 2 * m * 2)
+    ms = _time(lib, stream, a.reps)
+    print(json.dumps({"what": "bdgd_block_update", "m": m, "rows": n, "ms": ms, "tflops": flops / ms / 1e9}))
+    # reference: the same products as cuBLAS GEMMs (rows of the torch tensors are columns of the blocks)
+    Sx = torch.cat([blk["X"], blk["P"], blk["W"]])
+    Sa = torch.cat([blk["AX"], blk["AP"], blk["AW"]])
+    cur = torch.cuda.current_stream()
+
+    def blas():
+        torch.mm(Cx, Sx, out=out["XN"])
+        torch.mm(Cx, Sa, out=out["AXN"])
+        torch.mm(Cp, Sx[m:], out=out["PN"])
+        torch.mm(Cp, Sa[m:], out=out["APN"])
+
+    ms2 = _time(blas, cur, a.reps)
+    print(json.dumps({"what": "cublas_fp64_same_products", "m": m, "rows": n, "ms": ms2, "tflops": flops / ms2 / 1e9}))
+    # projection shape: P -= X Cs, AP -= AX Cs (k = m, beta = 1), two outputs
+    Cs = torch.randn(m, m, dtype=torch.float64, device="cuda")
+    pouts = [(out["PN"].data_ptr(), m, -1.0, 1.0, [(blk["X"].data_ptr(), m, Cs.data_ptr(), m)]),
+             (out["APN"].data_ptr(), m, -1.0, 1.0, [(blk["AX"].data_ptr(), m, Cs.data_ptr(), m)])]
+
+    def libp():
+        rc = dc.block_update(0, False, n, n, pouts)
+        if rc:
+            raise RuntimeError(f"bdgd_block_update: {rc}")
+
+    pflops = 2.0 * n * m * m * 2
+    ms = _time(libp, stream, a.reps)
+    print(json.dumps({"what": "bdgd_block_update_projection", "m": m, "rows": n, "ms": ms,
+                      "tflops": pflops / ms / 1e9}))
+
+    def blasp():
+        out["PN"].addmm_(Cs, blk["X"], alpha=-1.0)
+        out["APN"].addmm_(Cs, blk["AX"], alpha=-1.0)
+
+    ms2 = _time(blasp, cur, a.reps)
+    print(json.dumps({"what": "cublas_fp64_projection", "m": m, "rows": n, "ms": ms2, "tflops": pflops / ms2 / 1e9}))
+    # agreement of the two on the last outputs
+    lib()
+    torch.cuda.synchronize()
+    ref = torch.mm(Cp, Sa[m:])
+    err = float((out["APN"] - ref).abs().max() / ref.abs().max())
+    print(json.dumps({"what": "max_rel_diff_APN", "value": err}))
     return 0
 
 

@@ -141,6 +141,33 @@ typedef struct {
 int bdgd_gram_tasks(bdgd_ctx *ctx, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                     double *d_out);
 
+/* Block update (no counterpart in the reference; it replaces the BLAS-3
+ * basis updates of the external solver): for each of `nout` outputs,
+ *   Y = alpha * sum_b S_b C_b + beta * Y
+ * with S_b n x k_b (column-major, leading dimension ld, 16-byte aligned),
+ * C_b a k_b x ncol device matrix (column-major, leading dimension ldc >= k_b,
+ * any alignment of FP64), Y n x ncol (leading dimension ld).  Up to 4
+ * outputs of up to 3 terms each, at most 16 column tiles of 64 in all, in
+ * one launch; beta == 0 does not read Y, and an output whose terms all have
+ * k_b = 0 is left untouched.  Y must not overlap any S_b.  Real
+ * FP64 only (FP64 tensor cores); other precisions, complex data or a layout
+ * outside these limits return BDGD_ERR_UNSUPPORTED without launching. */
+typedef struct {
+  const void *s;
+  const double *c;
+  int k, ldc;
+} bdgd_update_term;
+
+typedef struct {
+  void *y;
+  int ncol, nterm;
+  double alpha, beta;
+  bdgd_update_term term[3];
+} bdgd_update_out;
+
+int bdgd_block_update(bdgd_ctx *ctx, int prec, int cplx, uint64_t n, uint64_t ld, int nout,
+                      const bdgd_update_out *outs);
+
 /* Gram contraction that allocates nothing (no counterpart in the reference).
  *
  * Same inputs and output as bdgd_gram (Guu, Gvv, Guv, Ga of a block S and
