@@ -17,6 +17,7 @@
 #include <string.h>
 #include <time.h>
 
+#include "bdg/bdg_cuda.h"
 #include "bdg/bdg_internal.h"
 
 #ifndef M_PI
@@ -153,6 +154,62 @@ static void fill_planewave(bdg_t *bdg, void *S) {
     }
   }
   safe_free((void **)&kv);
+}
+
+/* The same block generated on the device (bdg_initd.cu): 0 when d_S (n x
+ * sizeSub, leading dim n, FP64 or FP32 per prec) was filled, 1 when the
+ * mode needs the host fill (CUSTOM, or REUSE with a stored buffer), < 0 on
+ * a device error. */
+int bdg_fill_initial_block_device(bdg_t *bdg, void *d_S, int prec) {
+  matmul_ctx_t *ctx = bdg->ctx;
+  if (ctx == NULL || ctx->dev == NULL) return 1;
+  const uint64_t n = 2 * ctx->size, m = bdg->sizeSub;
+  const int cplx = bdg->complex_psi0;
+  if (bdg->init_mode == BDG_INIT_CUSTOM) return 1;
+  if (bdg->init_mode == BDG_INIT_REUSE && bdg->reuse_buf && bdg->reuse_n == n && bdg->reuse_cols == m) return 1;
+  /* the |psi0| weights: the operators upload psi0 only when the dipolar term
+   * needs it, so bring the current one to the device here */
+  if (ctx->wf) {
+    const int rc = bdgd_set_wavefunction(ctx->dev, ctx->wf);
+    if (rc) return rc;
+  }
+  switch (bdg->init_mode) {
+    case BDG_INIT_CUSTOM:
+      return 1;
+    case BDG_INIT_REUSE:
+      if (bdg->reuse_buf && bdg->reuse_n == n && bdg->reuse_cols == m) return 1;
+      /* fall through */
+    case BDG_INIT_WF_WEIGHTED: {
+      uint32_t seed = 42;
+      if (!cplx) {
+        seed = (uint32_t)time(NULL);
+        if (seed == 0) seed = 1;
+      }
+      return bdgd_init_block(ctx->dev, prec, 1, seed, (int)m, NULL, d_S, n);
+    }
+    case BDG_INIT_PLANEWAVE:
+    default: {
+      const bdg_geom_hint_t hint =
+          bdg->custom_init_param ? (bdg_geom_hint_t)(intptr_t)bdg->custom_init_param : BDG_GEOM_AUTO;
+      uint64_t nk = 0;
+      kvec_t *kv = enumerate_kvecs(ctx, hint, (m + 1) / 2, &nk);
+      f64 *cols = xcalloc(4 * m, sizeof(f64));
+      for (uint64_t j = 0; j < m; j++) {
+        const uint64_t kvi = (j + 1) / 2;
+        if (kvi >= nk) continue; /* kind 0: noise column */
+        cols[4 * j] = (j % 2 == 1) ? 2.0 : 1.0;
+        for (uint64_t d = 0; d < ctx->dim; d++) {
+          const uint64_t kd = kv[kvi].idx[d];
+          const int64_t f = kd <= ctx->N[d] / 2 ? (int64_t)kd : (int64_t)kd - (int64_t)ctx->N[d];
+          cols[4 * j + 1 + d] = 2.0 * M_PI * (f64)f / ctx->L[d];
+        }
+      }
+      safe_free((void **)&kv);
+      const int rc = bdgd_init_block(ctx->dev, prec, 0, 42u, (int)m, cols, d_S, n);
+      free(cols);
+      return rc;
+    }
+  }
 }
 
 void bdg_fill_initial_block(bdg_t *bdg, void *S) {

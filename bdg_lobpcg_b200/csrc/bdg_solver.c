@@ -1056,10 +1056,20 @@ static int solve_gpu(bdg_t *bdg) {
   const int deflate = bdg->deflate && !cplx && ctx->wf;
   w->deflate = 0;
   if (deflate && (rc = goldstone_setup(w, dev, ctx, w->prec))) return rc;
-  /* initial block: host fill, upload (converted for FP32) */
+  /* initial block: generated on the device for the built-in modes; host
+   * fill and upload (converted for FP32) for CUSTOM and a stored REUSE
+   * buffer, or with BDG_HOST_INIT=1 */
+  int host_init = 1;
+  if (!getenv("BDG_HOST_INIT")) {
+    host_init = bdg_fill_initial_block_device(bdg, w->blk[NB_X], w->prec);
+    if (host_init < 0) {
+      fprintf(stderr, "bdg_solve: device initial block failed (%d): %s\n", host_init, bdgd_last_error());
+      return host_init;
+    }
+  }
   const size_t hesz = cplx ? sizeof(c64) : sizeof(f64);
   const size_t xb = n * m * hesz;
-  if (w->hX0_bytes != xb) {
+  if (host_init && w->hX0_bytes != xb) {
     if (w->hX0) cudaFreeHost(w->hX0);
     w->hX0 = NULL;
     w->hX0_bytes = 0;
@@ -1070,26 +1080,30 @@ static int solve_gpu(bdg_t *bdg) {
       w->hX0_bytes = xb;
     }
   }
-  const int pinned = w->hX0 != NULL;
-  void *X0 = pinned ? w->hX0 : xmalloc(xb);
-  /* a custom init fills every entry; the other modes rely on a zeroed block */
-  if (bdg->init_mode != BDG_INIT_CUSTOM) memset(X0, 0, xb);
-  bdg_fill_initial_block(bdg, X0);
-  if (mixed) {
-    void *tmp = NULL;
-    if ((rc = dmalloc(w, &tmp, xb))) return rc;
-    if (pinned) CUDA_TRY(cudaMemcpyAsync(tmp, X0, xb, cudaMemcpyHostToDevice, st));
-    else TRY(staged_copy(w, tmp, X0, xb, 1));
-    DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    dfree(w, tmp);
-  } else if (pinned) {
-    CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, xb, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+  if (host_init) {
+    const int pinned = w->hX0 != NULL;
+    void *X0 = pinned ? w->hX0 : xmalloc(xb);
+    /* a custom init fills every entry; the other modes rely on a zeroed block */
+    if (bdg->init_mode != BDG_INIT_CUSTOM) memset(X0, 0, xb);
+    bdg_fill_initial_block(bdg, X0);
+    if (mixed) {
+      void *tmp = NULL;
+      if ((rc = dmalloc(w, &tmp, xb))) return rc;
+      if (pinned) CUDA_TRY(cudaMemcpyAsync(tmp, X0, xb, cudaMemcpyHostToDevice, st));
+      else TRY(staged_copy(w, tmp, X0, xb, 1));
+      DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      dfree(w, tmp);
+    } else if (pinned) {
+      CUDA_TRY(cudaMemcpyAsync(w->blk[NB_X], X0, xb, cudaMemcpyHostToDevice, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+    } else {
+      TRY(staged_copy(w, w->blk[NB_X], X0, xb, 1));
+    }
+    if (!pinned) free(X0);
   } else {
-    TRY(staged_copy(w, w->blk[NB_X], X0, xb, 1));
+    CUDA_TRY(cudaStreamSynchronize(st));
   }
-  if (!pinned) free(X0);
   const double anorm = anorm_estimate(ctx);
   double *lam = xcalloc(3 * m, sizeof(double));
   double *res = xcalloc(nev, sizeof(double));

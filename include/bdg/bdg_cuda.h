@@ -168,6 +168,20 @@ typedef struct {
 int bdgd_block_update(bdgd_ctx *ctx, int prec, int cplx, uint64_t n, uint64_t ld, int nout,
                       const bdgd_update_out *outs);
 
+/* Initial iLOBPCG block on the device (no counterpart in the reference,
+ * which fills it on the host, src/solver.c:68-259 and :321-414): columns
+ * 0..ncols-1 of d_S (2*size rows, leading dimension ld, FP64 or FP32 per
+ * prec, complex when the context is), u = v.  mode 0: plane-wave columns,
+ * cols_host = ncols x {kind, fx, fy, fz} (kind 0 noise, 1 cos, 2 sin;
+ * f the angular wave numbers), value (wave + 1e-4 (xrand - 0.5)) |psi0| or
+ * (xrand - 0.5) |psi0|, one xorshift32 draw per element; mode 1:
+ * |sqrt(-2 log u1) cos(2 pi u2)| |psi0|, two draws per element.  The draws
+ * follow one xorshift32 stream from `seed` (nonzero), column after column,
+ * row after row, so the block equals the reference's host fill with the same
+ * seed up to the rounding of sin, cos, log and sqrt. */
+int bdgd_init_block(bdgd_ctx *ctx, int prec, int mode, uint32_t seed, int ncols, const double *cols_host, void *d_S,
+                    uint64_t ld);
+
 /* Gram contraction that allocates nothing (no counterpart in the reference).
  *
  * Same inputs and output as bdgd_gram (Guu, Gvv, Guv, Ga of a block S and

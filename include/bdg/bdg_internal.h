@@ -218,6 +218,12 @@ void bdg_ctx_apply_host(matmul_ctx_t *ctx, int op, const void *x, void *y,
                         uint64_t ncol, const char *caller);
 /* Fill the initial block S (n x sizeSub, host) per bdg->init_mode. */
 void bdg_fill_initial_block(bdg_t *bdg, void *S);
+/* The same block generated on the device into d_S (n x sizeSub, leading dim
+ * n; FP64 or FP32 per prec, complex on the _z path): 0 when filled, 1 when
+ * the mode needs the host fill (CUSTOM, or REUSE with a stored buffer), < 0
+ * on a device error.  The wavefunction must be on the device
+ * (bdg_device_context). */
+int bdg_fill_initial_block_device(bdg_t *bdg, void *d_S, int prec);
 
 #ifdef __cplusplus
 }
