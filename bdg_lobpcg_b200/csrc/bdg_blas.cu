@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "bdg_dev.h"
@@ -178,6 +179,11 @@ template <> struct GStage<double, false> { typedef double E; static constexpr in
 template <> struct GStage<float, false> { typedef float E; static constexpr int RK = 32, LDE = 36; };
 template <> struct GStage<double, true> { typedef double2 E; static constexpr int RK = 16, LDE = 18; };
 template <> struct GStage<float, true> { typedef float2 E; static constexpr int RK = 16, LDE = 18; };
+// stage shapes per kernel variant: V = 0 the shapes above; V = 1 half-height
+// stages (half the shared memory, so four 128-thread blocks fit an SM)
+template <typename T, bool CPLX, int V> struct GStageV : GStage<T, CPLX> {};
+template <typename T> struct GStageV<T, false, 1> { typedef typename GStage<T, false>::E E; static constexpr int RK = 16, LDE = 20; };
+template <typename T> struct GStageV<T, true, 1> { typedef typename GStage<T, true>::E E; static constexpr int RK = 8, LDE = 10; };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -195,11 +201,11 @@ template <typename E> __device__ __forceinline__ double im_of(E v) { return 0.0;
 template <> __device__ __forceinline__ double im_of<double2>(double2 v) { return v.y; }
 template <> __device__ __forceinline__ double im_of<float2>(float2 v) { return (double)v.y; }
 
-template <typename T, bool CPLX>
-__device__ __forceinline__ void stage_async(typename GStage<T, CPLX>::E *sm, const T *__restrict__ base, long long ld,
+template <typename T, bool CPLX, int V = 0>
+__device__ __forceinline__ void stage_async(typename GStageV<T, CPLX, V>::E *sm, const T *__restrict__ base, long long ld,
                                             int c0, int kc, long long r0, long long rend) {
-  typedef typename GStage<T, CPLX>::E E;
-  constexpr int RK = GStage<T, CPLX>::RK, LDE = GStage<T, CPLX>::LDE;
+  typedef typename GStageV<T, CPLX, V>::E E;
+  constexpr int RK = GStageV<T, CPLX, V>::RK, LDE = GStageV<T, CPLX, V>::LDE;
   constexpr int EB = (int)sizeof(E);
   constexpr int RPC = 16 / EB;          // rows per 16-byte chunk
   constexpr int CPC = RK / RPC;         // chunks per column
@@ -367,11 +373,11 @@ __device__ __forceinline__ void gram_tile_of(const GTask &tk, int local, int &ti
 
 // One tile of A^H B over rows [rbeg, rend): the two-stage cp.async pipeline
 // of k_gram_tasks2; writes the GT x GT partial to out (column-major, tile-local).
-template <typename T, bool CPLX>
+template <typename T, bool CPLX, int V = 0>
 __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, long long rbeg, long long rend,
-                                               double *__restrict__ out, typename GStage<T, CPLX>::E *buf) {
-  typedef typename GStage<T, CPLX>::E E;
-  constexpr int RK = GStage<T, CPLX>::RK, LDE = GStage<T, CPLX>::LDE;
+                                               double *__restrict__ out, typename GStageV<T, CPLX, V>::E *buf) {
+  typedef typename GStageV<T, CPLX, V>::E E;
+  constexpr int RK = GStageV<T, CPLX, V>::RK, LDE = GStageV<T, CPLX, V>::LDE;
   constexpr int ES = CPLX ? 2 : 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wi = warp & 1, wj = warp >> 1;
@@ -388,8 +394,8 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
   const T *B = (const T *)tk.b;
   const long long nst = rend > rbeg ? (rend - rbeg + RK - 1) / RK : 0;
   if (nst > 0) {
-    stage_async<T, CPLX>(buf, A, tk.lda, ti * GT, tk.ka, rbeg, rend);
-    stage_async<T, CPLX>(buf + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg, rend);
+    stage_async<T, CPLX, V>(buf, A, tk.lda, ti * GT, tk.ka, rbeg, rend);
+    stage_async<T, CPLX, V>(buf + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg, rend);
     cp_async_commit();
   }
   for (long long s = 0; s < nst; ++s) {
@@ -397,8 +403,8 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
     if (s + 1 < nst) {
       E *nxt = buf + ((s + 1) & 1) * 2 * GT * LDE;
       const long long r0 = rbeg + (s + 1) * RK;
-      stage_async<T, CPLX>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
-      stage_async<T, CPLX>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
+      stage_async<T, CPLX, V>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
+      stage_async<T, CPLX, V>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
       cp_async_commit();
       cp_async_wait<1>();
     } else {
@@ -452,9 +458,9 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
       }
 }
 
-template <typename T, bool CPLX>
-__global__ void __launch_bounds__(128) k_gram_sk(GArgsSK g) {
-  typedef typename GStage<T, CPLX>::E E;
+template <typename T, bool CPLX, int V>
+__global__ void __launch_bounds__(128, V ? 4 : 1) k_gram_sk(GArgsSK g) {
+  typedef typename GStageV<T, CPLX, V>::E E;
   constexpr int ES = CPLX ? 2 : 1;
   extern __shared__ __align__(16) unsigned char gsm3[];
   E *buf = (E *)gsm3;
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(128) k_gram_sk(GArgsSK g) {
     const int tau = tk.tile0 + lt;
     const long long first = (tk.wbase + (long long)lt * tk.rowsP) / g.per;
     const int slot = g.segbase[tau] + (int)((long long)blockIdx.x - first);
-    gram_tile_rows<T, CPLX>(tk, ti, tj, r0, r1, g.part + (long long)slot * GT * GT * ES, buf);
+    gram_tile_rows<T, CPLX, V>(tk, ti, tj, r0, r1, g.part + (long long)slot * GT * GT * ES, buf);
     pos += seglen;
   }
 }
@@ -523,14 +529,14 @@ __global__ void k_gram_sk_reduce(GArgsSK g, int cplx, int ldo, double *__restric
 }
 
 // resident blocks of k_gram_sk<T, CPLX> on this device (cached per device)
-template <typename T, bool CPLX>
+template <typename T, bool CPLX, int V>
 static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
   static int cached[64];
   const int dev = c->device < 64 ? c->device : 63;
   if (cached[dev]) return cached[dev];
   int nsm = 0, nb = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX>, 128, sm) != cudaSuccess || nb < 1 ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX, V>, 128, sm) != cudaSuccess || nb < 1 ||
       nsm < 1) {
     cudaGetLastError();
     return 148;
@@ -541,13 +547,14 @@ static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
 
 // Stream-K launch of the task list; returns BDGD_ERR_UNSUPPORTED when the
 // tile count exceeds GMAXTILES (the caller then uses the row-split kernels).
-template <typename T, bool CPLX>
+template <typename T, bool CPLX, int V>
 static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, double *d_out) {
-  typedef typename GStage<T, CPLX>::E E;
+  typedef typename GStageV<T, CPLX, V>::E E;
   const int es = cplx ? 2 : 1;
   if (ga.ntiles > GMAXTILES) return BDGD_ERR_UNSUPPORTED;
-  const size_t sm = sizeof(E) * 2 * 2 * GT * GStage<T, CPLX>::LDE;
-  if (sm > 48 * 1024) BDGD_CK(cudaFuncSetAttribute(k_gram_sk<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const size_t sm = sizeof(E) * 2 * 2 * GT * GStageV<T, CPLX, V>::LDE;
+  if (sm > 48 * 1024)
+    BDGD_CK(cudaFuncSetAttribute(k_gram_sk<T, CPLX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   static thread_local GArgsSK g;  // large; host-side staging of the kernel parameters
   memset(&g, 0, sizeof g);
   g.nt = ga.nt;
@@ -562,7 +569,7 @@ static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, doubl
     W += (long long)nti * t.rowsP;
   }
   if (W == 0) return BDGD_OK;
-  const int slots = gram_sk_slots<T, CPLX>(c, sm);
+  const int slots = gram_sk_slots<T, CPLX, V>(c, sm);
   long long per = (W + slots - 1) / slots;
   per = (per + GSK_STEP - 1) / GSK_STEP * GSK_STEP;
   const long long nblk = (W + per - 1) / per;
@@ -584,7 +591,7 @@ static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, doubl
   if (rc) return rc;
   g.part = c->gram_part;
   bdgd_count_launch();
-  k_gram_sk<T, CPLX><<<(unsigned)nblk, 128, sm, c->stream>>>(g);
+  k_gram_sk<T, CPLX, V><<<(unsigned)nblk, 128, sm, c->stream>>>(g);
   BDGD_CK(cudaGetLastError());
   bdgd_count_launch();
   k_gram_sk_reduce<<<dim3(32, g.nt), 256, 0, c->stream>>>(g, cplx, ldo, d_out);
@@ -704,10 +711,15 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
         aligned = false;
   }
   if (aligned && !getenv("BDG_GRAM_SPLIT")) {
-    if (prec == BDGD_F32) rc = cplx ? launch_gram_sk<float, true>(c, g, cplx, ldo, d_out)
-                                    : launch_gram_sk<float, false>(c, g, cplx, ldo, d_out);
-    else rc = cplx ? launch_gram_sk<double, true>(c, g, cplx, ldo, d_out)
-                   : launch_gram_sk<double, false>(c, g, cplx, ldo, d_out);
+    // real FP64: half-height stages, four blocks per SM (BDG_GRAM_VARIANT=0 for
+    // the full-height stages at three blocks per SM)
+    const char *gv = getenv("BDG_GRAM_VARIANT");
+    const bool half = !(gv && gv[0] == '0');
+    if (prec == BDGD_F32) rc = cplx ? launch_gram_sk<float, true, 0>(c, g, cplx, ldo, d_out)
+                                    : launch_gram_sk<float, false, 0>(c, g, cplx, ldo, d_out);
+    else if (cplx) rc = launch_gram_sk<double, true, 0>(c, g, cplx, ldo, d_out);
+    else rc = half ? launch_gram_sk<double, false, 1>(c, g, cplx, ldo, d_out)
+                   : launch_gram_sk<double, false, 0>(c, g, cplx, ldo, d_out);
     if (rc != BDGD_ERR_UNSUPPORTED) return rc;
   }
   if (aligned) {
@@ -1248,17 +1260,16 @@ extern "C" int bdgd_set_ritz_block(bdgd_ctx *c, double *Ga, double *Guv, int ldo
 // Gram.  One launch serves up to UMAXO outputs, each a sum of up to three
 // terms, so X, AX, P, AP of the update step come out of one pass.  Tiles: 64
 // rows x 64 output columns per 128-thread block (four warps of 32 x 32), the
-// contraction walked in 32-column stages through a two-stage cp.async
-// pipeline: the S stage as [32 columns][64 rows] (16-byte copies along the
-// contiguous rows), the small matrix C as [64 output columns][32] (8-byte
-// copies, it may have any leading dimension).  Products on the FP64 tensor
-// cores (mma.sync m8n8k4).  Consecutive blocks take the output column tiles
-// of one row tile, so S tiles shared by several outputs are read from L2.
+// contraction walked in 16-column stages through a cp.async ring: the S
+// stage as [16 columns][64 rows] (16-byte copies along the contiguous rows),
+// the small matrix C as [64 output columns][16] (8-byte copies, it may have
+// any leading dimension).  Products on the FP64 tensor cores (mma.sync
+// m8n8k4).  The blocks are persistent; each takes the output column tasks of
+// its row tiles in turn, so S tiles shared by several outputs come from L2.
 // ---------------------------------------------------------------------------
 #define UMAXO 4
 #define UMAXCT 16
 #define UKC 16   // contraction columns per stage
-#define USTG 4   // stages in the cp.async ring
 #define ULDM 68  // S stage row: 64 rows + 4 (the 16 fragment addresses of a half-warp fall in distinct banks)
 #define ULDK 20  // C stage row: UKC + 4
 
@@ -1318,11 +1329,13 @@ __device__ __forceinline__ int upd_nst(const UArgs &u, int ct) {
 
 // Persistent: block b takes row tiles b, b + grid, ... and, for each, the
 // column tasks 0..nct-1 in turn (their S tiles are shared through L2); all
-// stages run through one USTG-deep cp.async ring, so the loads of a tile's
+// stages run through one USTG-deep cp.async ring (USTG = 2: double
+// buffering, the next stage loading while one is multiplied), so the loads of a tile's
 // first stages overlap the previous tile's last products and its stores.
 // With beta != 0 the accumulators start at (beta / alpha) Y, loaded together
 // at the start of the tile (exact for the solver's alpha = +-1, beta = 1).
-__global__ void __launch_bounds__(128, 3) k_block_update(UArgs u, long long nrt) {
+template <int USTG, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_block_update(UArgs u, long long nrt) {
   extern __shared__ __align__(16) unsigned char usm[];
   double *buf = (double *)usm;  // [USTG][A: UKC x ULDM | B: 64 x ULDK]
   constexpr int STG = UKC * ULDM + 64 * ULDK;
@@ -1411,7 +1424,8 @@ __global__ void __launch_bounds__(128, 3) k_block_update(UArgs u, long long nrt)
   cp_async_wait<0>();
 }
 
-// resident blocks of k_block_update on this device (queried once per device)
+// resident blocks of a k_block_update variant on this device (queried once per device)
+template <int USTG, int MINB>
 static int upd_slots(size_t sm) {
   static int cache[64];
   int dev = 0;
@@ -1419,11 +1433,26 @@ static int upd_slots(size_t sm) {
   if (dev < 0 || dev >= 64) dev = 0;
   if (cache[dev] <= 0) {
     int nb = 0, nsm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_block_update, 128, sm) != cudaSuccess || nb < 1) nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_block_update<USTG, MINB>, 128, sm) != cudaSuccess ||
+        nb < 1)
+      nb = 1;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
     cache[dev] = nb * nsm;
   }
   return cache[dev];
+}
+
+template <int USTG, int MINB>
+static int launch_update(bdgd_ctx *c, const UArgs &u, long long nrt) {
+  const size_t sm = sizeof(double) * USTG * (UKC * ULDM + 64 * ULDK);
+  if (!bdgd_capturing)
+    BDGD_CK(cudaFuncSetAttribute(k_block_update<USTG, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const long long slots = upd_slots<USTG, MINB>(sm);
+  const long long nblk = nrt < slots ? nrt : slots;
+  bdgd_count_launch();
+  k_block_update<USTG, MINB><<<(unsigned)nblk, 128, sm, c->stream>>>(u, nrt);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
 }
 
 extern "C" int bdgd_block_update(bdgd_ctx *c, int prec, int cplx, uint64_t n, uint64_t ld, int nout,
@@ -1464,11 +1493,9 @@ extern "C" int bdgd_block_update(bdgd_ctx *c, int prec, int cplx, uint64_t n, ui
   if (nct == 0) return BDGD_OK;
   u.nct = nct;
   const long long nrt = ((long long)n + 63) / 64;
-  const size_t sm = sizeof(double) * USTG * (UKC * ULDM + 64 * ULDK);
-  if (!bdgd_capturing) BDGD_CK(cudaFuncSetAttribute(k_block_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const long long nblk = nrt < upd_slots(sm) ? nrt : upd_slots(sm);
-  bdgd_count_launch();
-  k_block_update<<<(unsigned)nblk, 128, sm, c->stream>>>(u, nrt);
-  BDGD_CK(cudaGetLastError());
-  return BDGD_OK;
+  // double-buffered stages at four blocks per SM (12.8 against 13.5 ms for the
+  // 128^3 basis update); BDG_UPDATE_VARIANT=4: four-deep ring, three blocks per SM
+  const char *v = getenv("BDG_UPDATE_VARIANT");
+  if (v && v[0] == '4') return launch_update<4, 3>(c, u, nrt);
+  return launch_update<2, 4>(c, u, nrt);
 }
