@@ -379,8 +379,13 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
   typedef typename GStageV<T, CPLX, V>::E E;
   constexpr int RK = GStageV<T, CPLX, V>::RK, LDE = GStageV<T, CPLX, V>::LDE;
   constexpr int ES = CPLX ? 2 : 1;
+  // SPLIT (complex, V = 2, 256 threads): warps 0-3 accumulate the real parts
+  // and warps 4-7 the imaginary parts of the same four 32 x 32 quadrants, one
+  // accumulator set per warp
+  constexpr bool SPLIT = CPLX && V == 2;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wi = warp & 1, wj = warp >> 1;
+  const int part = SPLIT ? (warp >> 2) : 0;
+  const int wi = warp & 1, wj = (warp >> 1) & 1;
   const int lr = lane & 3, lc = lane >> 2;
   double acc[4][4][2], aci[4][4][2];
 #pragma unroll
@@ -427,19 +432,39 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
         br[nj] = re_of<E>(v);
         bi[nj] = im_of<E>(v);
       }
+      if constexpr (SPLIT) {
+        if (part == 0) {
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
+          for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-        for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
-      if (CPLX) {
+            for (int nj = 0; nj < 4; ++nj) {
+              dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+              dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
+            }
+        } else {
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < 4; ++nj) {
+              dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], bi[nj]);
+              dmma(acc[mi][nj][0], acc[mi][nj][1], -ai[mi], br[nj]);
+            }
+        }
+      } else {
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-          for (int nj = 0; nj < 4; ++nj) {
-            dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
-            dmma(aci[mi][nj][0], aci[mi][nj][1], ar[mi], bi[nj]);
-            dmma(aci[mi][nj][0], aci[mi][nj][1], -ai[mi], br[nj]);
-          }
+          for (int nj = 0; nj < 4; ++nj) dmma(acc[mi][nj][0], acc[mi][nj][1], ar[mi], br[nj]);
+        if (CPLX) {
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < 4; ++nj) {
+              dmma(acc[mi][nj][0], acc[mi][nj][1], ai[mi], bi[nj]);
+              dmma(aci[mi][nj][0], aci[mi][nj][1], ar[mi], bi[nj]);
+              dmma(aci[mi][nj][0], aci[mi][nj][1], -ai[mi], br[nj]);
+            }
+        }
       }
     }
     __syncthreads();
@@ -453,13 +478,21 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
         const int il = wi * 32 + mi * 8 + lc;
         const int jl = wj * 32 + nj * 8 + 2 * lr + e;
         const long long o = ((long long)jl * GT + il) * ES;
-        out[o] = acc[mi][nj][e];
-        if (CPLX) out[o + 1] = aci[mi][nj][e];
+        if constexpr (SPLIT) {
+          out[o + part] = acc[mi][nj][e];
+        } else {
+          out[o] = acc[mi][nj][e];
+          if (CPLX) out[o + 1] = aci[mi][nj][e];
+        }
       }
 }
 
+// threads per block of a k_gram_sk variant (V = 2 splits real and imaginary
+// accumulation over twice the warps)
+template <int V> constexpr int gram_threads() { return V == 2 ? 256 : 128; }
+
 template <typename T, bool CPLX, int V>
-__global__ void __launch_bounds__(128, V ? 4 : 1) k_gram_sk(GArgsSK g) {
+__global__ void __launch_bounds__(gram_threads<V>(), V == 1 ? 4 : (V == 2 ? 2 : 1)) k_gram_sk(GArgsSK g) {
   typedef typename GStageV<T, CPLX, V>::E E;
   constexpr int ES = CPLX ? 2 : 1;
   extern __shared__ __align__(16) unsigned char gsm3[];
@@ -536,7 +569,7 @@ static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
   if (cached[dev]) return cached[dev];
   int nsm = 0, nb = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX, V>, 128, sm) != cudaSuccess || nb < 1 ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX, V>, gram_threads<V>(), sm) != cudaSuccess || nb < 1 ||
       nsm < 1) {
     cudaGetLastError();
     return 148;
@@ -591,7 +624,7 @@ static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, doubl
   if (rc) return rc;
   g.part = c->gram_part;
   bdgd_count_launch();
-  k_gram_sk<T, CPLX, V><<<(unsigned)nblk, 128, sm, c->stream>>>(g);
+  k_gram_sk<T, CPLX, V><<<(unsigned)nblk, gram_threads<V>(), sm, c->stream>>>(g);
   BDGD_CK(cudaGetLastError());
   bdgd_count_launch();
   k_gram_sk_reduce<<<dim3(32, g.nt), 256, 0, c->stream>>>(g, cplx, ldo, d_out);
@@ -715,9 +748,12 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
     // the full-height stages at three blocks per SM)
     const char *gv = getenv("BDG_GRAM_VARIANT");
     const bool half = !(gv && gv[0] == '0');
+    // complex FP64: real and imaginary parts on separate warps (29.8 against
+    // 28.9 TF/s at 128^3, k = 192; in FP32 the one-warp form is faster)
     if (prec == BDGD_F32) rc = cplx ? launch_gram_sk<float, true, 0>(c, g, cplx, ldo, d_out)
                                     : launch_gram_sk<float, false, 0>(c, g, cplx, ldo, d_out);
-    else if (cplx) rc = launch_gram_sk<double, true, 0>(c, g, cplx, ldo, d_out);
+    else if (cplx) rc = half ? launch_gram_sk<double, true, 2>(c, g, cplx, ldo, d_out)
+                             : launch_gram_sk<double, true, 0>(c, g, cplx, ldo, d_out);
     else rc = half ? launch_gram_sk<double, false, 1>(c, g, cplx, ldo, d_out)
                    : launch_gram_sk<double, false, 0>(c, g, cplx, ldo, d_out);
     if (rc != BDGD_ERR_UNSUPPORTED) return rc;

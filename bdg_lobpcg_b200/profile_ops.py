@@ -139,23 +139,29 @@ def gram_main(a):
 
     k, S = a.gram, a.grid ** 3
     n = 2 * S
-    dt = torch.float32 if a.prec else torch.float64
-    dc = B.DeviceContext(3, [a.grid] * 3, [24.0] * 3, False)
+    if a.complex:
+        dt = torch.complex64 if a.prec else torch.complex128
+    else:
+        dt = torch.float32 if a.prec else torch.float64
+    dc = B.DeviceContext(3, [a.grid] * 3, [24.0] * 3, a.complex)
     X = torch.randn(k, n, dtype=dt, device="cuda")
     AX = torch.randn(k, n, dtype=dt, device="cuda")
-    out = torch.zeros(4 * k * k, dtype=torch.float64, device="cuda")
+    out = torch.zeros(4 * k * k * (2 if a.complex else 1), dtype=torch.float64, device="cuda")
     stream = torch.cuda.ExternalStream(dc.stream)
 
     def lib():
-        dc.gram_ptr(a.prec, False, S, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr())
+        dc.gram_ptr(a.prec, a.complex, S, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr())
 
     ms = _time(lib, stream, a.reps)
     tiles = (k + 63) // 64
     symfrac = tiles * (tiles + 1) / 2 / (tiles * tiles)
-    flops_exec = 2.0 * S * k * k * (2 * symfrac + 1) + 2.0 * n * k * k
-    flops_min = 2.0 * S * k * k * 2 + 2.0 * n * k * k  # Guu, Gvv half each + Guv + Ga
-    print(json.dumps({"what": "bdgd_gram", "k": k, "rows": n, "prec": a.prec, "ms": ms,
+    cf = 4.0 if a.complex else 1.0  # real flops per complex multiply-add pair
+    flops_exec = cf * (2.0 * S * k * k * (2 * symfrac + 1) + 2.0 * n * k * k)
+    flops_min = cf * (2.0 * S * k * k * 2 + 2.0 * n * k * k)  # Guu, Gvv half each + Guv + Ga
+    print(json.dumps({"what": "bdgd_gram", "k": k, "rows": n, "prec": a.prec, "complex": a.complex, "ms": ms,
                       "tflops_executed": flops_exec / ms / 1e9, "tflops_useful": flops_min / ms / 1e9}))
+    if a.complex:
+        return 0
     Xd, AXd = X.double(), AX.double()
     cur = torch.cuda.current_stream()
     ms2 = _time(lambda: (torch.mm(Xd, Xd.t()), torch.mm(Xd, AXd.t())), cur, a.reps)
