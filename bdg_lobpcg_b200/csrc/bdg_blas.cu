@@ -1529,9 +1529,11 @@ extern "C" int bdgd_block_update(bdgd_ctx *c, int prec, int cplx, uint64_t n, ui
   if (nct == 0) return BDGD_OK;
   u.nct = nct;
   const long long nrt = ((long long)n + 63) / 64;
-  // double-buffered stages at four blocks per SM (12.8 against 13.5 ms for the
-  // 128^3 basis update); BDG_UPDATE_VARIANT=4: four-deep ring, three blocks per SM
+  // four-deep ring at three blocks per SM: inside the 128^3 solve its update
+  // stage took 778 ms against 822 ms for the double-buffered ring at four
+  // blocks per SM (BDG_UPDATE_VARIANT=2), although the latter times faster
+  // alone (12.8 against 13.5 ms per update)
   const char *v = getenv("BDG_UPDATE_VARIANT");
-  if (v && v[0] == '4') return launch_update<4, 3>(c, u, nrt);
-  return launch_update<2, 4>(c, u, nrt);
+  if (v && v[0] == '2') return launch_update<2, 4>(c, u, nrt);
+  return launch_update<4, 3>(c, u, nrt);
 }

@@ -38,6 +38,9 @@ from bdg_lobpcg_b200 import problems  # noqa: E402
 
 METRIC = "time to res<=1e-8, 32 BdG modes @128^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# DRAM read + write bytes per column of a real Lrep apply, summed over the
+# five pass kernels of one 8-column launch captured with ncu (128^3 FP64)
+LREP_DRAM_BYTES_PER_COLUMN = {(128, "f64"): 480.4e6}
 
 
 def load_peaks():
@@ -193,6 +196,49 @@ def run_reference(args, cfg):
     return 0
 
 
+def gram_roofline(B, torch, cfg, reps=5):
+    """The dominant kernel: the FP64 Gram contraction (k_gram_sk, DMMA) at the
+    solve's shapes (k = 3 sizeSub columns of S and AS on 2 N^3 rows: Guu, Gvv,
+    Guv, Ga), timed with CUDA events on the library's stream, against cuBLAS
+    FP64 GEMM 8192^3 measured in the same process (the FP64 tensor-core
+    reference; the measured-peaks file holds no FP64 figure)."""
+    size = int(np.prod(cfg["N"]))
+    n, k = 2 * size, 3 * cfg["sizeSub"]
+    dc = B.DeviceContext(3, cfg["N"], cfg["L"], False)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn(k, n, dtype=torch.float64, device="cuda", generator=gen)
+    AX = torch.randn(k, n, dtype=torch.float64, device="cuda", generator=gen)
+    out = torch.zeros(4 * k * k, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(dc.stream)
+
+    def timed(fn, st):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms = timed(lambda: dc.gram_ptr(0, False, size, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr()), stream)
+    tiles = (k + 63) // 64
+    symfrac = tiles * (tiles + 1) / 2 / (tiles * tiles)
+    flops = 2.0 * size * k * k * (2 * symfrac + 1) + 2.0 * n * k * k  # tiles computed
+    del X, AX
+    M = torch.randn(8192, 8192, dtype=torch.float64, device="cuda", generator=gen)
+    cur = torch.cuda.current_stream()
+    ms_ref = timed(lambda: torch.mm(M, M), cur)
+    ref = 2.0 * 8192 ** 3 / ms_ref / 1e9
+    dc.close()
+    achieved = flops / ms / 1e9
+    return {"bound": "tensor (FP64 DMMA)", "kernel": f"k_gram_sk: Gram of S, AS (k = {k}, rows = {n})",
+            "achieved": achieved, "peak": ref, "unit": "TFLOP/s", "frac": achieved / ref,
+            "peak_kind": "cuBLAS FP64 GEMM 8192^3 measured in this run", "ms_per_launch": ms,
+            "flops_per_launch": flops, "traffic": None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,7 +349,11 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "batched Lrep apply (5 FFT pass kernels)",
                      "achieved": a_gbs, "peak": peak, "unit": "GB/s",
                      "frac": (a_gbs / peak) if a_gbs else None, "peak_kind": peak_kind,
-                     "traffic": None, "precond_achieved": t_gbs},
+                     "algorithmic_bytes_per_column": lrep_bytes,
+                     "traffic": LREP_DRAM_BYTES_PER_COLUMN.get((cfg["N"][0], args.precision)),
+                     "traffic_basis": "DRAM bytes per column (ncu, 8-column launches of the five pass kernels)",
+                     "precond_achieved": t_gbs},
+        "roofline_gram": gram_roofline(B, torch, cfg) if args.precision == "f64" else None,
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": ck,
