@@ -16,10 +16,18 @@ between the two runs.
 R_TF is the Thomas-Fermi radius of the contact problem along the weakest
 trap axis: mu_TF = (15 g lambda / (4 pi))^(2/5) / 2 for the trap
 (1, 1, lambda) and a unit-norm condensate, R = sqrt(2 mu_TF) / min(1, lambda).
+
+Under torchrun (WORLD_SIZE > 1) the problems are sharded over the ranks,
+one GPU each, round robin (problem i on rank i mod world), with no exchange
+of solver data: every rank builds the same 64 configurations, solves its
+shard batched, and rank 0 gathers the per-problem records (host objects)
+and prints one JSON line whose time is the maximum over ranks of the time
+between device-wide synchronisations around the batched solves.
 """
 import argparse
 import json
 import math
+import os
 import sys
 import time
 
@@ -45,6 +53,68 @@ def sweep_configs(n, seed=3, nev=16):
     return out
 
 
+def shard(n, rank, world):
+    """Problem indices of one rank: rank, rank + world, ... (round robin, so
+    every rank gets a mix of the grid sizes)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"bad rank {rank} of {world}")
+    return list(range(rank, n, world))
+
+
+def merge_shards(n, parts):
+    """Per-rank lists of (problem index, record) -> the n records in problem
+    order; every index must come from exactly one rank."""
+    out = [None] * n
+    for part in parts:
+        for i, rec in part:
+            if not 0 <= i < n or out[i] is not None:
+                raise ValueError(f"problem {i} missing from the range or reported twice")
+            out[i] = rec
+    missing = [i for i, r in enumerate(out) if r is None]
+    if missing:
+        raise ValueError(f"problems {missing} not reported by any rank")
+    return out
+
+
+def distributed_main(a, world):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import bdg_lobpcg_b200 as B
+
+    rank = int(os.environ["RANK"])
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    cfgs = sweep_configs(a.problems, a.seed, a.nev)
+    mine = shard(len(cfgs), rank, world)
+    states = [problems.ground_state(B, cfgs[i]) for i in mine]
+    probs = [problems.build(B, cfgs[i], *st[:2], st[4], "f64")[0] for i, st in zip(mine, states)]
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    rcs, secs = B.solve_batch(probs, concurrency=a.concurrency, graphs=bool(a.graphs)) if probs else ([], [])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    recs = [(i, {"grid": cfgs[i]["N"][0], "rc": int(rc), "seconds": float(sec),
+                 "iterations": int(p.stats()["iterations"]), "eig0": float(p.eigenvalues()[0])})
+            for i, rc, sec, p in zip(mine, rcs, secs, probs)]
+    for p in probs:
+        p.close()
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object((wall, recs), gathered, dst=0)
+    if rank == 0:
+        t = max(g[0] for g in gathered)
+        merged = merge_shards(len(cfgs), [g[1] for g in gathered])
+        print(json.dumps({"problems": len(cfgs), "ranks": world, "scaling": "weak-by-problem",
+                          "seconds": t, "solves_per_s": len(cfgs) / t,
+                          "per_rank_seconds": [g[0] for g in gathered],
+                          "failed": [i for i, r in enumerate(merged) if r["rc"]], "per_problem": merged}))
+    dist.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--problems", type=int, default=64)
@@ -53,6 +123,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--nev", type=int, default=16)
     a = ap.parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        return distributed_main(a, world)
     import bdg_lobpcg_b200 as B
 
     cfgs = sweep_configs(a.problems, a.seed, a.nev)

@@ -196,6 +196,17 @@ def run_reference(args, cfg):
     return 0
 
 
+def max_over_ranks(values, dist, device):
+    """Per-rank timings reduced to their maximum over all ranks (every rank
+    calls this, in the same order; `device` is "cuda" under NCCL and "cpu"
+    under gloo)."""
+    import torch
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def gram_roofline(B, torch, cfg, reps=5):
     """The dominant kernel: the FP64 Gram contraction (k_gram_sk, DMMA) at the
     solve's shapes (k = 3 sizeSub columns of S and AS on 2 N^3 rows: Guu, Gvv,
@@ -306,9 +317,7 @@ def main():
     value = float(np.mean(dev_times))
     e2e = float(np.mean(e2e_times))
     if pg:
-        t = torch.tensor([value, e2e], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        value, e2e = float(t[0]), float(t[1])
+        value, e2e = max_over_ranks([value, e2e], pg, "cuda")
     if rank != 0:
         if pg:
             pg.destroy_process_group()
