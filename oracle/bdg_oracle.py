@@ -597,7 +597,8 @@ def svqb_coeffs(G, drop=1e-13):
 
 
 def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
-            criterion=CONV_BACKWARD, lock=True, drop=1e-13, verbose=False):
+            criterion=CONV_BACKWARD, lock=True, drop=1e-13, guard=1e-4, guard_strict=1e-12, stall_win=10,
+            verbose=False):
     """Block iLOBPCG for the pencil (A, B) = (diag(K, M), swap).
 
     X0: (m, n) block (rows are the columns of the reference's S), B-positive.
@@ -608,7 +609,11 @@ def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
       Rayleigh-Ritz on S = [X, P, W]  (rr_pencil)
       X <- S C,  P <- [P, W] C_pw  (restricted to the active columns)
     Active columns: wanted (j < nev) while their measure exceeds tol,
-    guards (j >= nev) while their backward error exceeds 1e-12.
+    guards (j >= nev) while their backward error exceeds the guard level:
+    `guard` (1e-4) while the worst backward error of the unconverged wanted
+    pairs keeps halving within every `stall_win` iterations, `guard_strict`
+    (1e-12) for the rest of the solve once it does not (loose guards can hold
+    the wanted pairs above tol, e.g. with an undeflated zero mode wanted).
     Converged when the measure is <= tol for each of the first nev pairs."""
     A = applyA or (lambda Z: matmulLrep(ctx, Z))
     T = applyT or (lambda Z: precondLrep(ctx, Z))
@@ -626,18 +631,26 @@ def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
     it = 0
     res = None
     nconv = 0
+    guard_now = guard
+    worst_hist = []
     while True:
         back = residual_measure(ctx, X, AX, lam, m, CONV_BACKWARD, anorm)
         res = back[:nev] if criterion == CONV_BACKWARD else \
             residual_measure(ctx, X, AX, lam, nev, criterion, anorm)
         nconv = int(np.sum(res <= tol))
+        unconv = res > tol
+        worst = float(np.max(back[:nev][unconv])) if np.any(unconv) else 0.0
+        worst_hist.append(worst)
+        if guard_now != guard_strict and len(worst_hist) > stall_win and \
+                not worst <= 0.5 * worst_hist[-1 - stall_win]:
+            guard_now = guard_strict
         history.append((lam[:nev].copy(), res.copy()))
         if verbose:
             print(it, lam[:nev], res.max())
         if nconv >= nev or it >= maxIter:
             break
         if lock:
-            act = np.concatenate([np.where(res > tol)[0], nev + np.where(back[nev:] > 1e-12)[0]])
+            act = np.concatenate([np.where(res > tol)[0], nev + np.where(back[nev:] > guard_now)[0]])
         else:
             act = np.arange(m)
         R = AX[act] - lam[act, None] * matmulSwap(ctx, X[act])
