@@ -25,6 +25,7 @@ and prints one JSON line whose time is the maximum over ranks of the time
 between device-wide synchronisations around the batched solves.
 """
 import argparse
+import faulthandler
 import json
 import math
 import os
@@ -116,6 +117,8 @@ def distributed_main(a, world):
 
 
 def main(argv=None):
+    # a crash in native code prints the Python stack of every thread
+    faulthandler.enable(all_threads=True)
     ap = argparse.ArgumentParser()
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--concurrency", type=int, default=8)
