@@ -141,6 +141,10 @@ def lib():
         "bdgd_apply_host": (i, [vp, i, vp, vp, u64]),
         "bdgd_gram": (i, [vp, i, i, u64, u64, vp, u64, vp, u64, vp]),
         "bdgd_block_update": (i, [vp, i, i, u64, u64, i, vp]),
+        "bdg_write_wavefunction_bin": (i, [vp, C.c_char_p]),
+        "bdg_write_modes_bin": (i, [vp, i, C.c_char_p]),
+        "bdg_write_eigenvalues_bin": (i, [vp, C.c_char_p]),
+        "bdg_load_wavefunction_bin": (i, [vp, C.c_char_p]),
         "bdg_lp_create": (i, [C.POINTER(vp), _u64p, i, i, i]),
         "bdg_lp_free": (None, [C.POINTER(vp)]),
         "bdg_lp_nparams": (u64, [vp]),
@@ -523,6 +527,20 @@ class Problem:
 
     def load_wavefunction(self, fn):
         return self._L.bdg_load_wavefunction(self._h, fn.encode())
+
+    # binary files (read them with bdg_lobpcg_b200.binio.read)
+    def write_wavefunction_bin(self, fn):
+        return self._L.bdg_write_wavefunction_bin(self._h, fn.encode())
+
+    def write_modes_bin(self, part, fn):
+        """part 0: u, 1: v (all nev modes)."""
+        return self._L.bdg_write_modes_bin(self._h, part, fn.encode())
+
+    def write_eigenvalues_bin(self, fn):
+        return self._L.bdg_write_eigenvalues_bin(self._h, fn.encode())
+
+    def load_wavefunction_bin(self, fn):
+        return self._L.bdg_load_wavefunction_bin(self._h, fn.encode())
 
 
 # ---------------------------------------------------------------------------

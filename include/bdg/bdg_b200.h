@@ -98,6 +98,38 @@ int bdg_solve_batch(bdg_t **problems, int n, int concurrency, int graphs, int *r
  * problem's set-up stay; the next bdg_solve reallocates them). */
 void bdg_release_device_memory(bdg_t *bdg);
 
+/* Binary files (no counterpart in the reference; its text files,
+ * src/io.c:13-165, stay as they are).  The text formats keep 8 significant
+ * digits and write one value per fprintf; these keep the exact doubles and
+ * write each array at once.  Layout: a 64-byte bdg_bin_header_t, then
+ * `count` consecutive fields of N[0]*N[1]*N[2] values each (f64, or
+ * interleaved re, im for c128), x fastest, in the host's byte order.
+ * Return codes as the text functions: 0 ok, -1 file error, -2 format or
+ * grid mismatch (or a bad `part`), -3 nothing to write. */
+#define BDG_BIN_MAGIC "BDGBIN01"
+#define BDG_BIN_VERSION 1u
+enum { BDG_BIN_WAVEFUNCTION = 0, BDG_BIN_MODES_U = 1, BDG_BIN_MODES_V = 2, BDG_BIN_EIGENVALUES = 3 };
+enum { BDG_BIN_F64 = 0, BDG_BIN_C128 = 1 };
+
+typedef struct {
+  char magic[8];     /* "BDGBIN01" */
+  uint32_t version;  /* BDG_BIN_VERSION */
+  uint32_t kind;     /* BDG_BIN_WAVEFUNCTION, _MODES_U, _MODES_V, _EIGENVALUES */
+  uint32_t dtype;    /* BDG_BIN_F64 or BDG_BIN_C128 */
+  uint32_t dim;      /* grid dimension; N[d] = 1 for d >= dim */
+  uint64_t N[3];
+  uint64_t count;    /* fields (1 for psi0, nev for modes); eigenvalues: nev values */
+  uint64_t reserved;
+} bdg_bin_header_t;
+
+int bdg_write_wavefunction_bin(const bdg_t *bdg, const char *filename);
+/* all nev modes of the last solve: part 0 = u, 1 = v */
+int bdg_write_modes_bin(const bdg_t *bdg, int part, const char *filename);
+int bdg_write_eigenvalues_bin(const bdg_t *bdg, const char *filename);
+/* psi0 from a file written by bdg_write_wavefunction_bin for the same grid
+ * and path (real or complex); as bdg_set_wavefunction afterwards */
+int bdg_load_wavefunction_bin(bdg_t *bdg, const char *filename);
+
 #ifdef __cplusplus
 }
 #endif
