@@ -218,3 +218,22 @@ def test_init_block_planewave_host(bdg):
     assert np.allclose(S[:, :16], S[:, 16:])
     assert np.allclose(S[0, :16], 1.0, atol=1e-4)  # k = 0 cos
     assert np.allclose(np.abs(S[1, :16]), np.abs(np.sin(x)), atol=1e-4)
+
+
+def test_public_headers_compile_as_c11_and_cpp(tmp_path):
+    """The C ABI headers compile as the reference compiles its sources
+    (-std=c11, Makefile:3) with -Wall -Wextra -pedantic -Werror, and as C++17."""
+    import shutil
+    import subprocess
+
+    if not shutil.which("gcc") or not shutil.which("g++"):
+        pytest.skip("no host compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = tmp_path / "hdr.c"
+    src.write_text("\n".join(f'#include "bdg/{h}"' for h in
+                             ("bdg.h", "bdg_b200.h", "bdg_cuda.h", "bdg_learn.h", "bdg_internal.h", "memory.h"))
+                   + "\nint main(void) { return 0; }\n")
+    for cmd in (["gcc", "-std=c11", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-I", inc, str(src)],
+                ["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-x", "c++", "-I", inc, str(src)]):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
