@@ -141,6 +141,7 @@ def lib():
         "bdgd_apply_host": (i, [vp, i, vp, vp, u64]),
         "bdgd_gram": (i, [vp, i, i, u64, u64, vp, u64, vp, u64, vp]),
         "bdgd_block_update": (i, [vp, i, i, u64, u64, i, vp]),
+        "bdg_set_initial_block": (i, [vp, vp, u64, u64]),
         "bdg_write_wavefunction_bin": (i, [vp, C.c_char_p]),
         "bdg_write_modes_bin": (i, [vp, i, C.c_char_p]),
         "bdg_write_eigenvalues_bin": (i, [vp, C.c_char_p]),
@@ -417,9 +418,15 @@ class Problem:
             self._L.bdg_set_init_mode(self._h, mode, None, C.c_void_p(param) if param else None)
 
     def set_initial_block(self, X):
-        """Custom initial block from an (m, n) array (u = v for B-positivity)."""
+        """Initial block from an (m, n) array (rows = columns of the block; u = v
+        for B-positivity), after set_solver_params.  The library borrows the
+        array (bdg_set_initial_block); this object keeps it alive."""
         X = np.ascontiguousarray(X, dtype=np.complex128 if self.cplx else np.float64)
-        self.set_init_mode(INIT_CUSTOM, lambda n, m: X)
+        m, n = X.shape
+        rc = self._L.bdg_set_initial_block(self._h, C.c_void_p(X.ctypes.data), n, m)
+        if rc:
+            raise ValueError(f"bdg_set_initial_block: block {m} x {n} does not fit the problem ({rc})")
+        self._x0 = X
 
     def reuse_modes(self, noise_frac):
         return self._L.bdg_reuse_modes(self._h, noise_frac)

@@ -89,6 +89,30 @@ void bdg_set_init_mode(bdg_t *bdg, bdg_init_mode_t mode, bdg_init_fn fn, void *p
   bdg->custom_init_param = param;
 }
 
+/* CUSTOM fill from the block given to bdg_set_initial_block */
+static void init_from_host_block(const bdg_t *bdg, void *X, uint64_t n, uint64_t sizeSub, void *param) {
+  (void)param;
+  const size_t esz = bdg->complex_psi0 ? sizeof(c64) : sizeof(f64);
+  if (bdg->init_block == NULL || n != bdg->init_block_n || sizeSub != bdg->init_block_m) {
+    fprintf(stderr, "bdg_solve: the block of bdg_set_initial_block is %llu x %llu, the solve needs %llu x %llu\n",
+            (unsigned long long)bdg->init_block_n, (unsigned long long)bdg->init_block_m, (unsigned long long)n,
+            (unsigned long long)sizeSub);
+    memset(X, 0, (size_t)(n * sizeSub) * esz);
+    return;
+  }
+  memcpy(X, bdg->init_block, (size_t)(n * sizeSub) * esz);
+}
+
+int bdg_set_initial_block(bdg_t *bdg, const void *X, uint64_t n, uint64_t sizeSub) {
+  BDG_REQUIRE(bdg, BDG_HAS_SYSTEM, "bdg_set_initial_block");
+  if (X == NULL || n != 2 * bdg->ctx->size || sizeSub == 0 || sizeSub != bdg->sizeSub) return -2;
+  bdg->init_block = X;
+  bdg->init_block_n = n;
+  bdg->init_block_m = sizeSub;
+  bdg_set_init_mode(bdg, BDG_INIT_CUSTOM, init_from_host_block, NULL);
+  return 0;
+}
+
 /* ---- setup (reference src/setup.c) ----------------------------------------- */
 void bdg_set_trap(bdg_t *bdg, f64 (*V_trap)(uint64_t dim, const f64 *r, const void *param), const void *param) {
   BDG_REQUIRE(bdg, BDG_HAS_SYSTEM, "bdg_set_trap");

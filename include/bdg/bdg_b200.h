@@ -98,6 +98,17 @@ int bdg_solve_batch(bdg_t **problems, int n, int concurrency, int graphs, int *r
  * problem's set-up stay; the next bdg_solve reallocates them). */
 void bdg_release_device_memory(bdg_t *bdg);
 
+/* Initial block from a host array (no counterpart in the reference, where
+ * a BDG_INIT_CUSTOM callback fills it): X is n x sizeSub, column-major
+ * (n = 2 * grid size, u rows then v rows; f64, or c64 on the complex
+ * path), after bdg_set_solver_params.  The library borrows X: it must stay
+ * valid and unchanged until the last bdg_solve that uses it (each solve
+ * copies it).  Same as bdg_set_init_mode(BDG_INIT_CUSTOM, ...) with a callback
+ * that copies X, but no caller code runs inside bdg_solve, which matters on
+ * the solver threads of bdg_solve_batch.  Returns 0, or -2 when X is NULL or
+ * the shape is not the problem's. */
+int bdg_set_initial_block(bdg_t *bdg, const void *X, uint64_t n, uint64_t sizeSub);
+
 /* Binary files (no counterpart in the reference; its text files,
  * src/io.c:13-165, stay as they are).  The text formats keep 8 significant
  * digits and write one value per fprintf; these keep the exact doubles and

@@ -162,6 +162,8 @@ struct bdg_t {
   uint64_t harvest_cap, harvest_n;
   int block_ws;             /* workspace holding the last solve's block (0/1), or -1 */
   size_t modes_bytes;       /* allocation size of modes_u / modes_v (reused across solves) */
+  const void *init_block;   /* caller's initial block (bdg_set_initial_block), borrowed */
+  uint64_t init_block_n, init_block_m;
 };
 
 /* ---- context lifecycle (reference src/bdg_internal.h:151-153) ------------ */

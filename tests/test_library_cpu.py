@@ -237,3 +237,34 @@ def test_public_headers_compile_as_c11_and_cpp(tmp_path):
                 ["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-x", "c++", "-I", inc, str(src)]):
         r = subprocess.run(cmd, capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_set_initial_block_borrowed(bdg, capfd):
+    """bdg_set_initial_block: the host fill copies the caller's block exactly
+    (real and complex); a shape that is not the problem's is refused (-2, a
+    ValueError in the binding); a sizeSub changed afterwards yields a zero
+    block and a message instead of reading past the caller's array."""
+    import ctypes as C
+
+    lib = bdg.lib()
+    lib.bdg_fill_initial_block.restype = None
+    lib.bdg_fill_initial_block.argtypes = [C.c_void_p, C.c_void_p]
+    for cplx in (False, True):
+        p = bdg.Problem(1, [8], [4.0], cplx)
+        p.set_system()
+        p.set_solver_params(2, 4, 10, 1e-6)
+        rng = np.random.default_rng(4)
+        X = rng.standard_normal((4, 16)) + (1j * rng.standard_normal((4, 16)) if cplx else 0)
+        p.set_initial_block(X)
+        out = np.zeros(X.size * (2 if cplx else 1))
+        lib.bdg_fill_initial_block(p._h, out.ctypes.data)
+        got = out.view(np.complex128) if cplx else out
+        assert np.array_equal(got.reshape(4, 16), X)
+        with pytest.raises(ValueError):
+            p.set_initial_block(X[:3])
+        p.set_solver_params(2, 5, 10, 1e-6)  # sizeSub no longer matches the borrowed block
+        out2 = np.full(16 * 5 * (2 if cplx else 1), 7.0)
+        lib.bdg_fill_initial_block(p._h, out2.ctypes.data)
+        assert np.all(out2 == 0.0)
+        assert "bdg_set_initial_block" in capfd.readouterr().err
+        p.close()
