@@ -3,7 +3,7 @@
 Each case restates one assertion block of pstuermer/BDG_LOBPCG tests/test_*.c
 (file:line in the docstring) as (setup, input, expected output, tolerance)
 and runs against an *adapter*: the CPU oracle (tests/test_oracle_cpu.py) or
-the GPU library (tests/test_known_answers_gpu.py).  Same inputs, same
+the GPU library (test_known_answer_gpu in tests/test_ops_gpu.py).  Same inputs, same
 tolerances as the reference (1e-10 absolute unless stated).
 """
 import math
