@@ -1365,9 +1365,9 @@ __device__ __forceinline__ int upd_nst(const UArgs &u, int ct) {
 
 // Persistent: block b takes row tiles b, b + grid, ... and, for each, the
 // column tasks 0..nct-1 in turn (their S tiles are shared through L2); all
-// stages run through one USTG-deep cp.async ring (USTG = 2: double
-// buffering, the next stage loading while one is multiplied), so the loads of a tile's
-// first stages overlap the previous tile's last products and its stores.
+// stages run through one USTG-deep cp.async ring (USTG - 1 stages loading
+// while one is multiplied), so the loads of a tile's first stages overlap the
+// previous tile's last products and its stores.
 // With beta != 0 the accumulators start at (beta / alpha) Y, loaded together
 // at the start of the tile (exact for the solver's alpha = +-1, beta = 1).
 template <int USTG, int MINB>
