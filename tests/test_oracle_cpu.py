@@ -89,3 +89,26 @@ def test_oracle_dense_known_answer_1d():
     r = O.ilobpcg(ctx, X0, 4, 300, 1e-10)
     assert r.converged >= 4
     assert np.allclose(r.eigvals[1:4], omega[1:4], rtol=1e-7)
+
+
+def test_oracle_dense_known_answer_3d():
+    """The oracle iLOBPCG on a 3D trapped dipolar problem (8^3, contact and
+    dipolar terms, mu below the spectrum so K and M are positive definite)
+    against the dense spectrum: omega = sqrt(eig(K M)) of the assembled
+    operators, five lowest modes to 1e-11 relative."""
+    N, L = [8, 8, 8], [6.0, 6.0, 6.0]
+    oc0 = O.Ctx(3, N, L)
+    O.set_system(oc0)
+    c = O.grid_coords(oc0)
+    Z, Y, X = np.meshgrid(c[2], c[1], c[0], indexing="ij")
+    psi = np.exp(-0.5 * (X ** 2 + Y ** 2 + 2 * Z ** 2)).reshape(-1)
+    psi /= math.sqrt(np.sum(psi ** 2) * np.prod([l / n for l, n in zip(L, N)]))
+    oc = O.build_problem(N, L, [1.0, 1.0, 1.5], 5.0, 2.0, psi, 0.2, Rc=3.0)
+    E = np.eye(oc.size)
+    Kd = O.matmulK(oc, E).T
+    Md = O.matmulM(oc, E).T
+    assert np.abs(Kd - Kd.T).max() < 1e-12 and np.abs(Md - Md.T).max() < 1e-12
+    omega = np.sqrt(np.sort(np.linalg.eigvals(Kd @ Md).real)[:5])
+    r = O.ilobpcg(oc, O.gaussian_block_bpositive(oc, 10, 1), 5, 400, 1e-11)
+    assert r.converged >= 5
+    assert np.all(np.abs(r.eigvals[:5] - omega) / omega < 1e-11), (r.eigvals[:5], omega)
