@@ -112,3 +112,30 @@ def test_oracle_dense_known_answer_3d():
     r = O.ilobpcg(oc, O.gaussian_block_bpositive(oc, 10, 1), 5, 400, 1e-11)
     assert r.converged >= 5
     assert np.all(np.abs(r.eigvals[:5] - omega) / omega < 1e-11), (r.eigvals[:5], omega)
+
+
+def test_oracle_dense_known_answer_3d_complex():
+    """The complex (_z) oracle path on the same 8^3 problem with psi0 carrying
+    a global phase e^{0.3 i}: K and M are Hermitian, and the iLOBPCG modes
+    equal the dense sqrt(eig(K M)) and the real problem's spectrum."""
+    N, L = [8, 8, 8], [6.0, 6.0, 6.0]
+    oc0 = O.Ctx(3, N, L)
+    O.set_system(oc0)
+    c = O.grid_coords(oc0)
+    Z, Y, X = np.meshgrid(c[2], c[1], c[0], indexing="ij")
+    psi = np.exp(-0.5 * (X ** 2 + Y ** 2 + 2 * Z ** 2)).reshape(-1)
+    psi /= math.sqrt(np.sum(psi ** 2) * np.prod([l / n for l, n in zip(L, N)]))
+    spectra = []
+    for cplx in (False, True):
+        oc = O.build_problem(N, L, [1.0, 1.0, 1.5], 5.0, 2.0, psi * (np.exp(0.3j) if cplx else 1.0), 0.2, Rc=3.0,
+                             complex_psi0=cplx)
+        E = np.eye(oc.size, dtype=complex if cplx else float)
+        Kd = O.matmulK(oc, E).T
+        Md = O.matmulM(oc, E).T
+        assert np.abs(Kd - Kd.conj().T).max() < 1e-12 and np.abs(Md - Md.conj().T).max() < 1e-12
+        omega = np.sqrt(np.sort(np.linalg.eigvals(Kd @ Md).real)[:5])
+        r = O.ilobpcg(oc, O.gaussian_block_bpositive(oc, 10, 1), 5, 400, 1e-11)
+        assert r.converged >= 5
+        assert np.all(np.abs(r.eigvals[:5] - omega) / omega < 1e-11)
+        spectra.append(omega)
+    assert np.allclose(spectra[0], spectra[1], rtol=1e-12)
