@@ -481,9 +481,10 @@ class SolveResult:
 
 def goldstone_projector(ctx, tol=1e-13, maxit=5000):
     """B-orthogonal projector onto the complement of the Goldstone Jordan
-    chain {[psi0; 0], [0; w]} with M w = psi0 (real psi0).  Physical modes
-    with omega != 0 satisfy psi0^H v = 0 and w^H u = 0.  w is computed by CG
-    on M."""
+    chain {[psi0; 0], [0; w]} with M w = psi0.  Physical modes with
+    omega != 0 satisfy psi0^H v = 0 and w^H u = 0.  w is computed by CG on M
+    (Hermitian positive definite).  Holds for complex psi0 too, wherever
+    K psi0 = 0; w^H psi0 = psi0^H M^-1 psi0 is real."""
     S = ctx.size
     psi = ctx.wf.astype(ctx.ctype)
     w = cg(lambda z: matmulM(ctx, z), psi, tol=tol, maxit=maxit)
