@@ -11,9 +11,10 @@ the complex Gram, with the same spectrum as the real problem.  The
 singly quantised vortex of the configuration is not produced here (see the
 design notes: the library's ground-state producer is real, and the vortex's
 anomalous mode makes the BdG pencil indefinite, outside the definite-pencil
-iLOBPCG).  Convergence is the backward error (no Goldstone deflation on the
-complex path); the true residual ||K M v - w^2 v|| / ||v|| of the result is
-reported.  Prints one JSON line per precision.
+iLOBPCG).  Convergence is the backward error without Goldstone deflation
+(so the Goldstone mode is among the results); the true residual
+||K M v - w^2 v|| / ||v|| of the nonzero modes is reported.  Prints one JSON
+line per precision.
 """
 import argparse
 import json

@@ -628,11 +628,32 @@ static int rayleigh_ritz(ws_t *w, bdgd_ctx *dev, int k, int m, double drop, doub
   return 0;
 }
 
-/* ---- deflation of the Goldstone chain (real psi0) -------------------------- */
+/* ---- deflation of the Goldstone chain ---------------------------------------
+ * x <- x - a [psi0; 0] - b [0; w] with a = w^H u / w^H psi0 and
+ * b = psi0^H v / psi0^H w (w^H psi0 = psi0^H M^-1 psi0 is real), so that
+ * w^H u = 0 and psi0^H v = 0.  Complex blocks: the gemv with the conjugate
+ * transpose gives conj(a) w^H psi0, and gerc conjugates it back. */
 static int deflate_block(ws_t *w, bdgd_ctx *dev, void *V, int q) {
   if (!w->deflate || q <= 0) return 0;
   const int S = (int)w->S, n = (int)w->n;
-  if (w->prec == BDGD_F32) {
+  if (w->cplx && w->prec == BDGD_F32) {
+    const cuComplex *psi = (const cuComplex *)w->defl, *wv = psi + S;
+    cuComplex *coef = (cuComplex *)w->wtmp;
+    const cuComplex one = {1.f, 0.f}, zero = {0.f, 0.f}, c1 = {(float)(-1.0 / w->wpsi), 0.f};
+    BLAS_TRY(cublasCgemv(w->blas, CUBLAS_OP_C, S, q, &one, (const cuComplex *)V, n, wv, 1, &zero, coef, 1));
+    BLAS_TRY(cublasCgerc(w->blas, S, q, &c1, psi, 1, coef, 1, (cuComplex *)V, n));
+    BLAS_TRY(cublasCgemv(w->blas, CUBLAS_OP_C, S, q, &one, (const cuComplex *)V + S, n, psi, 1, &zero, coef, 1));
+    BLAS_TRY(cublasCgerc(w->blas, S, q, &c1, wv, 1, coef, 1, (cuComplex *)V + S, n));
+  } else if (w->cplx) {
+    const cuDoubleComplex *psi = (const cuDoubleComplex *)w->defl, *wv = psi + S;
+    cuDoubleComplex *coef = (cuDoubleComplex *)w->wtmp;
+    const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0}, c1 = {-1.0 / w->wpsi, 0.0};
+    BLAS_TRY(cublasZgemv(w->blas, CUBLAS_OP_C, S, q, &one, (const cuDoubleComplex *)V, n, wv, 1, &zero, coef, 1));
+    BLAS_TRY(cublasZgerc(w->blas, S, q, &c1, psi, 1, coef, 1, (cuDoubleComplex *)V, n));
+    BLAS_TRY(cublasZgemv(w->blas, CUBLAS_OP_C, S, q, &one, (const cuDoubleComplex *)V + S, n, psi, 1, &zero, coef,
+                         1));
+    BLAS_TRY(cublasZgerc(w->blas, S, q, &c1, wv, 1, coef, 1, (cuDoubleComplex *)V + S, n));
+  } else if (w->prec == BDGD_F32) {
     const float *psi = (const float *)w->defl, *wv = psi + S;
     float *coef = (float *)w->wtmp;
     const float one = 1.f, zero = 0.f, c1 = (float)(-1.0 / w->wpsi);
@@ -652,8 +673,61 @@ static int deflate_block(ws_t *w, bdgd_ctx *dev, void *V, int q) {
   return 0;
 }
 
+/* w = M^-1 psi0 by conjugate gradients, complex psi0 (M Hermitian positive
+ * definite; FP64, on the device). */
+static int goldstone_setup_z(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int prec) {
+  const int S = (int)w->S;
+  cuDoubleComplex *x, *r, *p, *q, *psi;
+  TRY(dmalloc(w, (void **)&x, 5 * (size_t)S * sizeof(cuDoubleComplex)));
+  r = x + S;
+  p = r + S;
+  q = p + S;
+  psi = q + S;
+  const size_t vb = (size_t)S * sizeof(cuDoubleComplex);
+  cudaStream_t st = stream_of(dev);
+  CUDA_TRY(cudaMemcpyAsync(psi, ctx->wf, vb, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(x, 0, vb, st));
+  CUDA_TRY(cudaMemcpyAsync(r, psi, vb, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(p, psi, vb, cudaMemcpyDeviceToDevice, st));
+  cuDoubleComplex d;
+  BLAS_TRY(cublasSetPointerMode(w->blas, CUBLAS_POINTER_MODE_HOST));
+  BLAS_TRY(cublasZdotc(w->blas, S, r, 1, r, 1, &d));
+  double rr = d.x;
+  const double bn = sqrt(rr);
+  for (int it = 0; it < 20000 && sqrt(rr) > 1e-13 * bn; it++) {
+    DEV_TRY(bdgd_apply(dev, BDGD_OP_M, BDGD_F64, p, (uint64_t)S, q, (uint64_t)S, 1));
+    BLAS_TRY(cublasZdotc(w->blas, S, p, 1, q, 1, &d));
+    const cuDoubleComplex al = {rr / d.x, 0.0}, nal = {-rr / d.x, 0.0};
+    BLAS_TRY(cublasZaxpy(w->blas, S, &al, p, 1, x, 1));
+    BLAS_TRY(cublasZaxpy(w->blas, S, &nal, q, 1, r, 1));
+    BLAS_TRY(cublasZdotc(w->blas, S, r, 1, r, 1, &d));
+    const double be = d.x / rr;
+    BLAS_TRY(cublasZdscal(w->blas, S, &be, p, 1));
+    const cuDoubleComplex one = {1.0, 0.0};
+    BLAS_TRY(cublasZaxpy(w->blas, S, &one, r, 1, p, 1));
+    rr = d.x;
+  }
+  BLAS_TRY(cublasZdotc(w->blas, S, x, 1, psi, 1, &d)); /* w^H psi0, real */
+  w->wpsi = d.x;
+  if (w->defl) dfree(w, w->defl);
+  w->defl = NULL;
+  TRY(dmalloc(w, (void **)&w->defl, 2 * vb));
+  if (prec == BDGD_F32) {
+    DEV_TRY(bdgd_convert(dev, 1, psi, w->defl, 2 * (uint64_t)S));
+    DEV_TRY(bdgd_convert(dev, 1, x, (float *)w->defl + 2 * (size_t)S, 2 * (uint64_t)S));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(w->defl, psi, vb, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync((cuDoubleComplex *)w->defl + S, x, vb, cudaMemcpyDeviceToDevice, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  dfree(w, x);
+  w->deflate = 1;
+  return 0;
+}
+
 /* w = M^-1 psi0 by conjugate gradients (FP64, on the device). */
 static int goldstone_setup(ws_t *w, bdgd_ctx *dev, const matmul_ctx_t *ctx, int prec) {
+  if (w->cplx) return goldstone_setup_z(w, dev, ctx, prec);
   const int S = (int)w->S;
   double *x, *r, *p, *q, *psi;
   TRY(dmalloc(w, (void **)&x, 5 * (size_t)S * sizeof(double)));
@@ -1076,7 +1150,7 @@ static int solve_gpu(bdg_t *bdg) {
   const int mixed = (bdg->precision == BDG_PREC_MIXED);
   ws_t *w = mixed ? &wsp[1] : &wsp[0];
   if ((rc = ws_setup(w, dev, S, m, nev, cplx, mixed ? BDGD_F32 : BDGD_F64))) return rc;
-  const int deflate = bdg->deflate && !cplx && ctx->wf;
+  const int deflate = bdg->deflate && ctx->wf;
   w->deflate = 0;
   if (deflate && (rc = goldstone_setup(w, dev, ctx, w->prec))) return rc;
   /* initial block: generated on the device for the built-in modes; host

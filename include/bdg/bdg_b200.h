@@ -54,8 +54,8 @@ typedef struct {
 void bdg_set_precision(bdg_t *bdg, int precision);
 void bdg_set_convergence(bdg_t *bdg, int criterion);
 /* Restrict the search to the B-orthogonal complement of the Goldstone
- * Jordan chain {[psi0; 0], [0; M^-1 psi0]} (real psi0 only), so the nev
- * wanted pairs are the lowest nonzero modes. */
+ * Jordan chain {[psi0; 0], [0; M^-1 psi0]} (real or complex psi0 with
+ * K psi0 = 0), so the nev wanted pairs are the lowest nonzero modes. */
 void bdg_set_goldstone_deflation(bdg_t *bdg, int enable);
 /* FP64 iterations appended to a BDG_PREC_MIXED solve (default 3 max). */
 void bdg_set_refinement(bdg_t *bdg, int max_iters);

@@ -161,3 +161,28 @@ def test_complex_path_matches_real(bdg):
     # skip the Goldstone pair (near 0) and compare the rest
     sel = d > 1e-2
     assert np.all(np.abs(d[sel] - z[sel]) < 1e-9 * np.abs(d[sel]) + 1e-9), (d, z)
+
+
+def test_goldstone_deflation_complex_psi0(bdg):
+    """Goldstone deflation on the complex path: the 16^3 stationary dipolar
+    ground state with a global phase e^{0.3 i} as complex psi0, true residual
+    <= 1e-8, gives the real deflated problem's four lowest nonzero modes
+    (1e-9 relative), and the same as the oracle's complex deflated solve."""
+    ev = []
+    for cplx in (False, True):
+        oc, p = _dipolar_problem(bdg, "gs16", cplx=cplx, phase=0.3)
+        X0 = O.gaussian_block_bpositive(oc, 8, 0)
+        p.set_solver_params(4, 8, 400, 1e-8)
+        p.set_initial_block(X0)
+        p.set_goldstone_deflation(True)
+        p.set_convergence(bdg.CONV_TRUE_RESIDUAL)
+        assert p.solve() == 0
+        assert p.converged() >= 4
+        assert p.stats()["max_true_residual"] <= 1e-8
+        ev.append(p.eigenvalues()[:4].copy())
+        if cplx:
+            proj, _ = O.goldstone_projector(oc)
+            ref = O.ilobpcg(oc, X0, 4, 400, 1e-8, proj=proj, criterion=O.CONV_TRUE_RESIDUAL)
+            assert np.all(np.abs(ev[-1] - ref.eigvals[:4]) / ref.eigvals[:4] < 1e-9)
+        p.close()
+    assert np.all(np.abs(ev[0] - ev[1]) / ev[0] < 1e-9)
