@@ -83,7 +83,10 @@ void bdg_set_solver_params(bdg_t *bdg, uint64_t nev, uint64_t sizeSub, uint64_t 
   bdg->tol = tol;
 }
 
+static void init_from_host_block(const bdg_t *bdg, void *X, uint64_t n, uint64_t sizeSub, void *param);
+
 void bdg_set_init_mode(bdg_t *bdg, bdg_init_mode_t mode, bdg_init_fn fn, void *param) {
+  if (fn != init_from_host_block) bdg->init_block = NULL; /* another init source replaces the stored block */
   bdg->init_mode = mode;
   bdg->custom_init_fn = fn;
   bdg->custom_init_param = param;

@@ -84,9 +84,9 @@ int bdg_solve_batch(bdg_t **problems, int n, int concurrency, int graphs, int *r
   b.secs = seconds_out;
   pthread_mutex_init(&b.mu, NULL);
   pthread_t *th = (pthread_t *)calloc((size_t)concurrency, sizeof(pthread_t));
-  int started = 0;
+  int started = 0; /* handles of the threads created, stored contiguously */
   for (int t = 0; t < concurrency; ++t)
-    if (pthread_create(&th[t], NULL, batch_worker, &b) == 0) started++;
+    if (pthread_create(&th[started], NULL, batch_worker, &b) == 0) started++;
   if (started == 0) batch_worker(&b); /* no threads available: solve here */
   for (int t = 0; t < started; ++t) pthread_join(th[t], NULL);
   free(th);

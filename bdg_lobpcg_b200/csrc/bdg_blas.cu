@@ -12,6 +12,8 @@
 // * residual / norm kernels and small-matrix helpers for the Rayleigh-Ritz
 //   step.
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -564,9 +566,9 @@ __global__ void k_gram_sk_reduce(GArgsSK g, int cplx, int ldo, double *__restric
 // resident blocks of k_gram_sk<T, CPLX> on this device (cached per device)
 template <typename T, bool CPLX, int V>
 static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
-  static int cached[64];
+  static std::atomic<int> cached[64];  // written by several solver threads: idempotent, atomic
   const int dev = c->device < 64 ? c->device : 63;
-  if (cached[dev]) return cached[dev];
+  if (const int v = cached[dev].load(std::memory_order_relaxed)) return v;
   int nsm = 0, nb = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gram_sk<T, CPLX, V>, gram_threads<V>(), sm) != cudaSuccess || nb < 1 ||
@@ -574,8 +576,8 @@ static int gram_sk_slots(bdgd_ctx *c, size_t sm) {
     cudaGetLastError();
     return 148;
   }
-  cached[dev] = nb * nsm;
-  return cached[dev];
+  cached[dev].store(nb * nsm, std::memory_order_relaxed);
+  return nb * nsm;
 }
 
 // Stream-K launch of the task list; returns BDGD_ERR_UNSUPPORTED when the
@@ -1146,7 +1148,7 @@ extern "C" int bdgd_gather_cols(bdgd_ctx *c, const double *In, int ldi, int rows
 static __device__ __align__(256) double g_gram_noalloc_scratch[BDGD_NOALLOC_SCRATCH_DOUBLES];
 
 #define BDGD_NOALLOC_MAX_DEVICES 64
-static double *g_noalloc_ptr[BDGD_NOALLOC_MAX_DEVICES];
+static std::atomic<double *> g_noalloc_ptr[BDGD_NOALLOC_MAX_DEVICES];
 
 // Device address of the scratch array on the current device, looked up once
 // per device (the host-side symbol is not a device address).
@@ -1463,19 +1465,19 @@ __global__ void __launch_bounds__(128, MINB) k_block_update(UArgs u, long long n
 // resident blocks of a k_block_update variant on this device (queried once per device)
 template <int USTG, int MINB>
 static int upd_slots(size_t sm) {
-  static int cache[64];
+  static std::atomic<int> cache[64];  // written by several solver threads: idempotent, atomic
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
-  if (cache[dev] <= 0) {
+  if (cache[dev].load(std::memory_order_relaxed) <= 0) {
     int nb = 0, nsm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_block_update<USTG, MINB>, 128, sm) != cudaSuccess ||
         nb < 1)
       nb = 1;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
-    cache[dev] = nb * nsm;
+    cache[dev].store(nb * nsm, std::memory_order_relaxed);
   }
-  return cache[dev];
+  return cache[dev].load(std::memory_order_relaxed);
 }
 
 template <int USTG, int MINB>

@@ -25,9 +25,13 @@
 
 /* ---- logging (reference src/bdg_log.h: errors exit with EXIT_FAILURE) --- */
 static int use_color(void) {
-  static int cached = -1;
-  if (cached < 0) cached = isatty(STDERR_FILENO);
-  return cached;
+  static int cached = -1; /* idempotent; atomic loads/stores as several threads may log */
+  int c = __atomic_load_n(&cached, __ATOMIC_RELAXED);
+  if (c < 0) {
+    c = isatty(STDERR_FILENO);
+    __atomic_store_n(&cached, c, __ATOMIC_RELAXED);
+  }
+  return c;
 }
 
 void bdg_fatal(const char *file, int line, const char *fmt, ...) {

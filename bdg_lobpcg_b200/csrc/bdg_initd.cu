@@ -72,15 +72,18 @@ static uint32_t mat_vec_h(const uint32_t *m, uint32_t v) {
   return r;
 }
 
+static XsJump build_jump_tables() {
+  XsJump J;
+  for (int i = 0; i < 32; ++i) J.m[0][i] = xs_step_h(1u << i);
+  for (int b = 1; b < 32; ++b)
+    for (int i = 0; i < 32; ++i) J.m[b][i] = mat_vec_h(J.m[b - 1], J.m[b - 1][i]);
+  return J;
+}
+
+// built once; a function-local static is initialised exactly once even when
+// several solver threads (bdg_solve_batch) reach it together
 static const XsJump &jump_tables() {
-  static XsJump J;
-  static int built = 0;
-  if (!built) {
-    for (int i = 0; i < 32; ++i) J.m[0][i] = xs_step_h(1u << i);
-    for (int b = 1; b < 32; ++b)
-      for (int i = 0; i < 32; ++i) J.m[b][i] = mat_vec_h(J.m[b - 1], J.m[b - 1][i]);
-    built = 1;
-  }
+  static const XsJump J = build_jump_tables();
   return J;
 }
 

@@ -21,6 +21,8 @@
 // other small primes).  Real fields use the r2c half spectrum (x extent
 // N/2+1) between passes, so the spectrum traffic is that of FFTW's r2c.
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -734,15 +736,14 @@ extern "C" int bdgd_create(bdgd_ctx **out, uint64_t dim, const uint64_t *N, cons
   }
   {
     // keep freed stream-ordered scratch in the device pool for reuse
-    static int pool_done[64];
-    if (c->device >= 0 && c->device < 64 && !pool_done[c->device]) {
+    static std::atomic<int> pool_done[64];  // several solver threads create contexts at once
+    if (c->device >= 0 && c->device < 64 && !pool_done[c->device].exchange(1)) {
       cudaMemPool_t pool;
       if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
       }
       cudaGetLastError();
-      pool_done[c->device] = 1;
     }
   }
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
@@ -1223,7 +1224,7 @@ struct bdgd_graph {
   unsigned long long nkern, stamp;
 };
 #define BDGD_MAX_GRAPHS 48
-static unsigned long long g_graph_clock = 0;
+static std::atomic<unsigned long long> g_graph_clock{0};  // LRU stamps from several threads
 
 static void graphs_clear(bdgd_ctx *c) {
   for (int i = 0; i < c->ngraphs; ++i)

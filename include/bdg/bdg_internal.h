@@ -206,6 +206,21 @@ void dipolar_add_meanfield_z(matmul_ctx_t *ctx);
  * or a negative device error. */
 int bdg_fft_execute(void *plan, const void *in, void *out);
 
+/* FFTW names for code that runs ctx->fwd_plan / ctx->bwd_plan through the
+ * FFTW execute calls, as the reference's tests do (tests/test_setup.c:208-271
+ * calls fftw_execute_dft{,_r2c,_c2r} on those fields): the three calls map
+ * onto bdg_fft_execute, so such code compiles unchanged against this header.
+ * Macros rather than exported functions, so the library exports no FFTW
+ * symbol; skipped when the real fftw3.h came first (its FFTW3_H guard) or
+ * with BDG_NO_FFTW_COMPAT. */
+#if !defined(FFTW3_H) && !defined(BDG_NO_FFTW_COMPAT)
+typedef double fftw_complex[2];
+typedef void *fftw_plan;
+#define fftw_execute_dft(p, in, out) ((void)bdg_fft_execute((p), (in), (out)))
+#define fftw_execute_dft_r2c(p, in, out) ((void)bdg_fft_execute((p), (in), (out)))
+#define fftw_execute_dft_c2r(p, in, out) ((void)bdg_fft_execute((p), (in), (out)))
+#endif
+
 /* ---- solver (reference :220-221) ----------------------------------------- */
 int bdg_solve_d(bdg_t *bdg);
 int bdg_solve_z(bdg_t *bdg);

@@ -29,6 +29,9 @@ PROBLEMS = {
     # dipolar trap of the 32^3 benchmark config: box [-8, 8)^3, lambda = 2,
     # g = 1000, eps_dd = 0.5, dipoles along z, R_c = 8
     "c1_32": ([32, 32, 32], [16.0, 16.0, 16.0], (1.0, 1.0, 2.0), 1000.0, 500.0, 8.0),
+    # the 64^3 grid of the mixed-precision config: box [-12, 12)^3,
+    # lambda = 2, g = 1000, eps_dd = 0.7, R_c = 8
+    "c2_64": ([64, 64, 64], [24.0, 24.0, 24.0], (1.0, 1.0, 2.0), 1000.0, 700.0, 8.0),
 }
 
 

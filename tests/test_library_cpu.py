@@ -21,6 +21,7 @@ def _declared_functions():
         src = open(os.path.join(ROOT, "include", fn)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"static inline[^{]*\{.*?\n\}", "", src, flags=re.S)
+        src = re.sub(r"^\s*#.*$", "", src, flags=re.M)  # macros (the FFTW-name compatibility)
         for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{]*)\)\s*;", src):
             name = m.group(1)
             if name in ("if", "while", "for", "sizeof", "return", "void", "int", "double") or name.startswith("BDG_"):
