@@ -141,6 +141,17 @@ typedef struct {
 int bdgd_gram_tasks(bdgd_ctx *ctx, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                     double *d_out);
 
+/* Integer tensor-core GEMM tile building block (no counterpart in the
+ * reference): D = A B^T with A (M x K) and B (N x K) int8, rows K-contiguous
+ * (leading dimensions in elements, multiples of 16, 16-byte aligned), D
+ * (M x N) int32 row-major with leading dimension ldd.  M a multiple of 128,
+ * N of 64, K of 32.  tcgen05 MMA (kind::i8) with the accumulator in tensor
+ * memory, on `stream` (a cudaStream_t).  *d_err (device int) is set to 1 if a
+ * wait on the tensor core timed out.  It exists so that the layouts of the
+ * FP64-emulation kernels are checked against exact integer arithmetic. */
+int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, const int8_t *B, uint64_t ldb, int32_t *D,
+                    uint64_t ldd, uint64_t M, uint64_t N, uint64_t K, int *d_err);
+
 /* Block update (no counterpart in the reference; it replaces the BLAS-3
  * basis updates of the external solver): for each of `nout` outputs,
  *   Y = alpha * sum_b S_b C_b + beta * Y

@@ -11,8 +11,14 @@ steps (newton_polish) to the exact discrete stationary state, so that
 K psi0 = 0 to ~1e-14 and the Goldstone mode is exact.
 
     python tests/golden/make_fixtures.py [name ...]
+    python tests/golden/make_fixtures.py solve <name> <nev> <seed> [threads]
 """
 import os
+
+# OpenBLAS worker threads otherwise spin between BLAS calls and starve the
+# OpenMP threads of the reference's CPU FFT (3x slower iterations on 8 cores);
+# read when the library loads, so set before numpy / scipy are imported
+os.environ.setdefault("OPENBLAS_THREAD_TIMEOUT", "4")
 import sys
 import time
 
@@ -45,11 +51,46 @@ def make(name):
     print(name, "mu_itp", mu_itp, "mu", mu, "|H psi - mu psi|", res, "steps", steps, "%.1fs" % (time.time() - t))
 
 
+def solve(name, nev, seed, threads=None):
+    """The FP64 CPU oracle solve of fixture `name` through the reference's
+    own solve path (oracle/_ref: bdg_solve -> src/solver.c -> restated
+    iLOBPCG on the reference operators): nev modes, sizeSub 2 nev, initial
+    block X0 ~ N(0, 1) with v = u at `seed`, true residual <= 1e-8, Goldstone
+    chain deflated.  Writes <name>_solve.npz: eigenvalues, iterations, the
+    per-iteration wall clock and the thread count."""
+    from oracle import ref as R
+
+    d = load(name)
+    N = [int(v) for v in d["N"]]
+    L = [float(v) for v in d["L"]]
+    om = [float(v) for v in d["omegas"]]
+    m = 2 * nev
+    threads = threads or os.cpu_count() or 1
+    R.set_threads(threads)
+    rp = R.build_problem(N, L, om, float(d["g"]), float(d["gdd"]), d["psi"], float(d["mu"]), Rc=float(d["rc"]))
+    size = int(np.prod(N))
+    u = np.random.default_rng(seed).standard_normal((m, size))
+    rp.set_solver_params(nev, m, 2000, 1e-8)
+    rp.set_initial_block(np.concatenate([u, u], axis=1))
+    t = time.time()
+    res = rp.solve(criterion=R.CONV_TRUE_RESIDUAL, deflate=True)
+    np.savez_compressed(os.path.join(HERE, f"{name}_solve.npz"), eigvals=res["eigvals"], iterations=res["iterations"],
+                        converged=res["converged"], timeline=res["timeline"], nev=nev, sizeSub=m, seed=seed,
+                        threads=threads)
+    print(name, "solve", res["iterations"], "iterations", res["converged"], "converged", "%.1fs" % (time.time() - t))
+    print(res["eigvals"])
+
+
 def load(name):
     d = np.load(os.path.join(HERE, f"{name}.npz"))
     return {k: d[k] for k in d.files}
 
 
 if __name__ == "__main__":
-    for nm in (sys.argv[1:] or list(PROBLEMS)):
-        make(nm)
+    args = sys.argv[1:]
+    if args[:1] == ["solve"]:
+        # python tests/golden/make_fixtures.py solve c2_64 16 1 [threads]
+        solve(args[1], int(args[2]), int(args[3]), int(args[4]) if len(args) > 4 else None)
+    else:
+        for nm in (args or list(PROBLEMS)):
+            make(nm)
