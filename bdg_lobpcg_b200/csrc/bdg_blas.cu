@@ -681,9 +681,22 @@ __global__ void k_gram_tasks_reduce(GArgs g, int cplx, int ldo, double *__restri
   }
 }
 
+extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out);
+
+// Tensor-core (int8 digits, tcgen05) FP64 Gram for real FP64 blocks: on with
+// BDG_GRAM_TC=1
+static bool gram_tc_on() {
+  const char *e = getenv("BDG_GRAM_TC");
+  return e && e[0] == '1';
+}
+
 extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                                double *d_out) {
   if (ntask <= 0) return BDGD_OK;
+  if (prec == BDGD_F64 && !cplx && gram_tc_on()) {
+    const int rc = bdgd_gram_oz(c, ntask, tasks, ldo, d_out);
+    if (rc != BDGD_ERR_UNSUPPORTED) return rc;
+  }
   if (ntask > GMAXT) {
     bdgd_set_error("bdgd_gram_tasks: at most %d tasks", GMAXT);
     return BDGD_ERR_ARG;

@@ -69,6 +69,8 @@ struct bdgd_ctx {
   size_t io_bytes;
   double *gram_part;
   size_t gram_part_bytes;
+  void *oz_buf;        // tensor-core Gram: column maxima of its operands + error flag (stream-ordered)
+  size_t oz_buf_bytes;
   size_t spec_cap;  // max scratch bytes per apply chunk
   double kin_dt;
   double *ptab;     // (1/size) / safe_val(mu + k^2/2) per spectrum point, for the current mu

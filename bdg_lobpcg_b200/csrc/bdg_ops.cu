@@ -823,7 +823,7 @@ extern "C" void bdgd_destroy(bdgd_ctx **pc) {
                   c->wf64,  c->wf32,  c->vdd,  c->ptab};
   for (void *b : bufs)
     if (b) cudaFree(b);
-  void *sbufs[] = {c->spec, c->io, c->gram_part};  // stream-ordered (bdgd_ensure)
+  void *sbufs[] = {c->spec, c->io, c->gram_part, c->oz_buf};  // stream-ordered (bdgd_ensure)
   for (void *b : sbufs)
     if (b) cudaFreeAsync(b, c->stream);
   if (c->stream) cudaStreamSynchronize(c->stream);
@@ -1238,9 +1238,9 @@ extern "C" int bdgd_trim(bdgd_ctx *c) {
   if (!c) return BDGD_ERR_ARG;
   BDGD_CK(cudaStreamSynchronize(c->stream));
   graphs_clear(c);
-  void **bufs[] = {&c->spec, &c->io, (void **)&c->gram_part};
-  size_t *sizes[] = {&c->spec_bytes, &c->io_bytes, &c->gram_part_bytes};
-  for (int i = 0; i < 3; ++i) {
+  void **bufs[] = {&c->spec, &c->io, (void **)&c->gram_part, &c->oz_buf};
+  size_t *sizes[] = {&c->spec_bytes, &c->io_bytes, &c->gram_part_bytes, &c->oz_buf_bytes};
+  for (int i = 0; i < 4; ++i) {
     if (*bufs[i]) BDGD_CK(cudaFreeAsync(*bufs[i], c->stream));
     *bufs[i] = nullptr;
     *sizes[i] = 0;

@@ -111,3 +111,449 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
       A, (long long)lda, B, (long long)ldb, D, (long long)ldd, (int)K, d_err);
   return bdgd_check(cudaGetLastError(), "k_tc_i8_gemm");
 }
+
+// ---------------------------------------------------------------------------
+// FP64 Gram contraction on the integer tensor cores (Ozaki-style splitting).
+//
+// C = A^T B over a long row range, A (rows x ka) and B (rows x kb) FP64,
+// column-major.  Each column c is scaled by a power of two 2^(55 - S_c) with
+// max_r |x_rc| < 2^(S_c - 1) (S_c from the column maximum, measured by a
+// pre-pass), rounded to a 54-bit integer X and written in 7 signed 8-bit
+// digits: X = sum_{t<6} d_t 256^t + d_6 256^6, taken from the bytes of
+// X + 0x808080808080 (the offset makes the six low digits signed).  Then
+//   sum_r a_r b_r = 2^(S_a + S_b - 110) sum_{t,u} 256^(t+u) sum_r d_t d'_u,
+// each inner sum an exact int32 dot product of int8 digits on the tensor
+// cores (tcgen05.mma kind::i8).  Diagonals t + u >= 5 are kept (34 MMAs per
+// 32-row step); the dropped ones are below 2^-57 of max|a| max|b| per row.
+// The 8 kept diagonals accumulate in 8 int32 TMEM accumulators (128 x 64
+// each, the whole 512 TMEM columns); a diagonal sums at most 7 products of
+// |d| <= 128 per row, so 16384 rows stay exact in int32.  Each work unit is
+// (task, 128 x 64 output tile, 16384-row chunk); its FP64 result goes to the
+// split partials that k_oz_reduce sums in a fixed order.
+// ---------------------------------------------------------------------------
+#define OZ_CHUNK 16384
+#define OZ_MAXT 48
+#define OZ_THREADS 256
+#define OZ_ND 7          // digits per value
+#define OZ_DMIN 5        // lowest kept diagonal t + u
+#define OZ_NDIAG 8       // kept diagonals 5..12
+#define OZ_P 55          // X = rint(a * 2^(OZ_P - S))
+#define OZ_STAGE_A (OZ_ND * 128 * 32)
+#define OZ_STAGE_B (OZ_ND * 64 * 32)
+#define OZ_STAGE (OZ_STAGE_A + OZ_STAGE_B)
+// dynamic shared memory: two stages plus bookkeeping, sized above half of an
+// SM's shared memory so that one CTA holds each SM (its TMEM is all taken)
+#define OZ_SMEM (120 * 1024)
+
+struct OzTask {
+  const double *a, *b;
+  long long lda, ldb, rows;
+  int ka, kb, out, i0, j0, sym, mirror;
+  int ta, tb, ntile, tile0;
+  int ma, mb;             // offsets of the operands' column maxima
+  long long part0;        // offset of the task's split partials (doubles)
+};
+
+struct OzArgs {
+  OzTask t[OZ_MAXT];
+  int nt, ntiles, nsplit;
+  const unsigned long long *colmax;  // |x| maxima as FP64 bit patterns
+  double *part;
+  int *err;
+};
+
+__device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale, int &S, bool &finite) {
+  const double m = __longlong_as_double((long long)bits);
+  finite = isfinite(m);
+  if (!(m > 0.0) || !finite) {  // zero column (or not finite: flagged at the flush)
+    scale = 1.0;
+    S = 0;
+    return;
+  }
+  int E = 0;
+  frexp(m, &E);  // m = f 2^E, f in [0.5, 1): |x| < 2^E
+  S = E + 1;
+  int p = OZ_P - S;
+  if (p > 1023) p = 1023;
+  if (p < -1022) p = -1022;
+  scale = ldexp(1.0, p);
+}
+
+// digits of 16 consecutive values (rows) -> per digit t one 16-byte vector
+__device__ __forceinline__ void oz_digits16(const double (&v)[16], double scale, uint4 (&dig)[OZ_ND]) {
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    uint32_t lo[4], hi[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long X = __double2ll_rn(v[4 * g + q] * scale) + 0x808080808080LL;
+      lo[q] = (uint32_t)X ^ 0x80808080u;
+      hi[q] = (uint32_t)((unsigned long long)X >> 32) ^ 0x8080u;
+    }
+    // 4 x 4 byte transposes: word t holds digit t of the four values
+    const uint32_t a0 = __byte_perm(lo[0], lo[1], 0x5140), a1 = __byte_perm(lo[2], lo[3], 0x5140);
+    const uint32_t a2 = __byte_perm(lo[0], lo[1], 0x7362), a3 = __byte_perm(lo[2], lo[3], 0x7362);
+    const uint32_t b0 = __byte_perm(hi[0], hi[1], 0x5140), b1 = __byte_perm(hi[2], hi[3], 0x5140);
+    const uint32_t b2 = __byte_perm(hi[0], hi[1], 0x7362), b3 = __byte_perm(hi[2], hi[3], 0x7362);
+    const uint32_t w[OZ_ND] = {__byte_perm(a0, a1, 0x5410), __byte_perm(a0, a1, 0x7632), __byte_perm(a2, a3, 0x5410),
+                               __byte_perm(a2, a3, 0x7632), __byte_perm(b0, b1, 0x5410), __byte_perm(b0, b1, 0x7632),
+                               __byte_perm(b2, b3, 0x5410)};
+#pragma unroll
+    for (int t = 0; t < OZ_ND; ++t) {
+      if (g == 0) dig[t].x = w[t];
+      if (g == 1) dig[t].y = w[t];
+      if (g == 2) dig[t].z = w[t];
+      if (g == 3) dig[t].w = w[t];
+    }
+  }
+}
+
+// 16 rows [r, r + 16) of one column, zero outside [.., rend) or for a column
+// outside the operand
+__device__ __forceinline__ void oz_load16(const double *__restrict__ col, long long r, long long rend, bool valid,
+                                          double (&v)[16]) {
+  if (valid && r + 16 <= rend) {
+    const double2 *p = reinterpret_cast<const double2 *>(col + r);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double2 x = __ldg(p + q);
+      v[2 * q] = x.x;
+      v[2 * q + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = (valid && r + q < rend) ? __ldg(col + r + q) : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk) {
+  extern __shared__ __align__(1024) uint8_t oz_smem[];
+  double *scaleA = reinterpret_cast<double *>(oz_smem + 2 * OZ_STAGE);
+  double *scaleB = scaleA + 128;
+  int *SA = reinterpret_cast<int *>(scaleB + 64);
+  int *SB = SA + 128;
+  int *badA = SB + 64;
+  int *badB = badA + 128;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(badB + 64);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // unit -> split, task, tile
+  const int split = blockIdx.x / g.ntiles;
+  int gt = blockIdx.x - split * g.ntiles;
+  int ti = 0;
+  while (ti + 1 < g.nt && g.t[ti + 1].tile0 <= gt) ++ti;
+  const OzTask &tk = g.t[ti];
+  int lt = gt - tk.tile0, ia = 0, jb = 0;
+  if (tk.sym) {  // tiles with 2 ia <= jb only (the rest comes from the transpose)
+    while (lt >= tk.tb - 2 * ia) {
+      lt -= tk.tb - 2 * ia;
+      ++ia;
+    }
+    jb = 2 * ia + lt;
+  } else {
+    ia = lt / tk.tb;
+    jb = lt - ia * tk.tb;
+  }
+  const long long r0 = (long long)split * chunk;
+  const long long r1 = min(tk.rows, r0 + chunk);
+  const int nsteps = r1 > r0 ? (int)((r1 - r0 + 31) / 32) : 0;
+
+  if (tid < 128) {
+    const int c = ia * 128 + tid;
+    double s = 1.0;
+    int S = 0;
+    bool fin = true;
+    if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin);
+    scaleA[tid] = s;
+    SA[tid] = S;
+    badA[tid] = !fin;
+  } else if (tid < 192) {
+    const int c = jb * 64 + tid - 128;
+    double s = 1.0;
+    int S = 0;
+    bool fin = true;
+    if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin);
+    scaleB[tid - 128] = s;
+    SB[tid - 128] = S;
+    badB[tid - 128] = !fin;
+  }
+  if (warp == 0 && nsteps > 0) tmem_alloc(tslot, 512);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = nsteps > 0 ? *tslot : 0u;
+
+  // this thread's columns: A column ca (all threads), B column cb (threads < 128)
+  const int ca = tid >> 1, ha = tid & 1;
+  const int cb = (tid & 127) >> 1, hb = tid & 1;
+  const bool hasB = tid < 128;
+  const bool va = ia * 128 + ca < tk.ka, vb = hasB && (jb * 64 + cb < tk.kb);
+  const double *colA = tk.a + (long long)(va ? ia * 128 + ca : 0) * tk.lda;
+  const double *colB = tk.b + (long long)(vb ? jb * 64 + cb : 0) * tk.ldb;
+  const double sa = scaleA[ca], sb = hasB ? scaleB[cb] : 1.0;
+  const int offA = (ca & 7) * 16 + (ca >> 3) * 256 + ha * 128;
+  const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + hb * 128;
+
+  double xa[16], xb[16];
+  if (nsteps > 0) {
+    oz_load16(colA, r0 + 16 * ha, r1, va, xa);
+    if (hasB) oz_load16(colB, r0 + 16 * hb, r1, vb, xb);
+  }
+  uint32_t ph[2] = {0u, 0u};
+  int failed = 0;
+  for (int ks = 0; ks < nsteps; ++ks) {
+    const int s = ks & 1;
+    // digits of this step from the registers, then the next step's loads
+    uint4 da[OZ_ND], db[OZ_ND];
+    oz_digits16(xa, sa, da);
+    if (hasB) oz_digits16(xb, sb, db);
+    if (ks + 1 < nsteps) {
+      const long long rn = r0 + (long long)(ks + 1) * 32;
+      oz_load16(colA, rn + 16 * ha, r1, va, xa);
+      if (hasB) oz_load16(colB, rn + 16 * hb, r1, vb, xb);
+    }
+    if (ks >= 2) {  // the MMAs committed two steps ago read this stage
+      const bool ok = mbar_wait(&bar[s], ph[s], TC_WAIT_LIMIT);
+      ph[s] ^= 1u;
+      failed = __syncthreads_or(!ok);
+      if (failed) break;
+    }
+    uint8_t *st = oz_smem + s * OZ_STAGE;
+#pragma unroll
+    for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(st + t * 4096 + offA) = da[t];
+    if (hasB) {
+#pragma unroll
+      for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(st + OZ_STAGE_A + t * 2048 + offB) = db[t];
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t id = idesc_i8(64);
+      const uint32_t base = smem_u32(st);
+#pragma unroll
+      for (int t = 0; t < OZ_ND; ++t)
+#pragma unroll
+        for (int u = 0; u < OZ_ND; ++u) {
+          const int D = t + u;
+          if (D < OZ_DMIN) continue;
+          const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+          mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
+                 smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
+        }
+      mma_commit(&bar[s]);
+    }
+  }
+  if (!failed && nsteps > 0) {  // the last commit covers all MMAs of the unit
+    const int s = (nsteps - 1) & 1;
+    const bool ok = mbar_wait(&bar[s], ph[s], TC_WAIT_LIMIT);
+    failed = __syncthreads_or(!ok);
+  }
+  tc_fence_after();
+  // flush: warp w reads TMEM lanes 32 (w % 4).., columns 32 (w / 4)..
+  const int row = 32 * (warp & 3) + lane;
+  const int i = ia * 128 + row;
+  const int kk = tk.ka * tk.kb;
+  double *part = g.part + tk.part0 + (long long)split * kk;
+  if (failed) {
+    if (tid == 0) atomicExch(g.err, 1);
+  } else {
+    for (int grp = 0; grp < 2; ++grp) {
+      const int c0 = 32 * (warp >> 2) + 16 * grp;
+      double acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+      if (nsteps > 0) {
+#pragma unroll
+        for (int d = 0; d < OZ_NDIAG; ++d) {
+          int32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
+          const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
+        }
+      }
+      if (i < tk.ka) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int j = jb * 64 + c0 + q;
+          if (j < tk.kb) {
+            double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
+            if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+            part[(long long)j * tk.ka + i] = val;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0 && nsteps > 0) tmem_free(tmem, 512);
+}
+
+// |x| maxima of the columns of an operand (FP64 bit patterns, atomic max;
+// the target starts at zero)
+__global__ void k_oz_colmax(const double *__restrict__ a, long long lda, long long rows, long long span,
+                            unsigned long long *__restrict__ out) {
+  const int c = blockIdx.x;
+  const long long rb = (long long)blockIdx.y * span, re = min(rows, rb + span);
+  const double *col = a + (long long)c * lda;
+  double m = 0.0;
+  for (long long r = rb + threadIdx.x; r < re; r += blockDim.x) {
+    const double x = fabs(__ldg(col + r));
+    m = (x > m || x != x) ? x : m;  // NaN propagates
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    const double y = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (y > m || y != y) ? y : m;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (red[w] > m || red[w] != red[w]) ? red[w] : m;
+    atomicMax(out + c, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// sum of the split partials in fixed order; symmetric tasks take the
+// transposed element where its tile was not computed; mirror writes C^T too
+__global__ void k_oz_reduce(OzArgs g, int ldo, double *__restrict__ outbuf) {
+  const OzTask &tk = g.t[blockIdx.y];
+  const long long kk = (long long)tk.ka * tk.kb;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < kk; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % tk.ka), j = (int)(q / tk.ka);
+    int si = i, sj = j;
+    if (tk.sym && 2 * (i / 128) > j / 64) {
+      si = j;
+      sj = i;
+    }
+    const double *pp = g.part + tk.part0 + (long long)sj * tk.ka + si;
+    double s = 0.0;
+    for (int sp = 0; sp < g.nsplit; ++sp) s += pp[(long long)sp * kk];
+    double *o = outbuf + (long long)tk.out * ldo * ldo;
+    o[(long long)(tk.j0 + j) * ldo + tk.i0 + i] = s;
+    if (tk.mirror) o[(long long)(tk.i0 + i) * ldo + tk.j0 + j] = s;
+  }
+}
+
+// Real FP64 task list on the tensor cores; BDGD_ERR_UNSUPPORTED (nothing
+// launched) for layouts outside the kernel's limits.
+extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out) {
+  if (ntask <= 0) return BDGD_OK;
+  if (ntask > OZ_MAXT) return BDGD_ERR_UNSUPPORTED;
+  OzArgs g;
+  memset(&g, 0, sizeof g);
+  g.nt = ntask;
+  // unique operands (pointer, leading dimension, rows, columns) -> column maxima
+  struct Op {
+    const double *p;
+    long long ld, rows;
+    int k, off;
+  } ops[2 * OZ_MAXT];
+  int nops = 0, moff = 0;
+  auto op_index = [&](const void *p, uint64_t ld, uint64_t rows, int k) -> int {
+    for (int i = 0; i < nops; ++i)
+      if (ops[i].p == p && ops[i].ld == (long long)ld && ops[i].rows == (long long)rows && ops[i].k == k)
+        return ops[i].off;
+    ops[nops] = {(const double *)p, (long long)ld, (long long)rows, k, moff};
+    moff += k;
+    return ops[nops++].off;
+  };
+  long long maxrows = 0;
+  int tiles = 0;
+  for (int i = 0; i < ntask; ++i) {
+    const bdgd_gram_task &s = tasks[i];
+    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0)
+      return BDGD_ERR_UNSUPPORTED;
+    OzTask &t = g.t[i];
+    t.a = (const double *)s.a;
+    t.b = (const double *)s.b;
+    t.lda = (long long)s.lda;
+    t.ldb = (long long)s.ldb;
+    t.rows = (long long)s.rows;
+    t.ka = s.ka;
+    t.kb = s.kb;
+    t.out = s.out;
+    t.i0 = s.i0;
+    t.j0 = s.j0;
+    t.sym = s.sym && s.ka == s.kb;  // a symmetric result: upper tiles computed
+    t.mirror = s.mirror;
+    t.ta = (s.ka + 127) / 128;
+    t.tb = (s.kb + 63) / 64;
+    if (t.sym) {
+      t.ntile = 0;
+      for (int a = 0; a < t.ta; ++a) t.ntile += t.tb - 2 * a > 0 ? t.tb - 2 * a : 0;
+    } else {
+      t.ntile = t.ta * t.tb;
+    }
+    t.tile0 = tiles;
+    tiles += t.ntile;
+    t.ma = op_index(s.a, s.lda, s.rows, s.ka);
+    t.mb = op_index(s.b, s.ldb, s.rows, s.kb);
+    if (t.rows > maxrows) maxrows = t.rows;
+  }
+  g.ntiles = tiles;
+  // row chunks: at most OZ_CHUNK rows (int32 exactness), enough units to fill the GPU
+  int nsplit = (2 * 148 + tiles - 1) / tiles;
+  const long long minsplit = (maxrows + OZ_CHUNK - 1) / OZ_CHUNK;
+  const long long maxsplit = (maxrows + 255) / 256;
+  if (nsplit < minsplit) nsplit = (int)minsplit;
+  if (nsplit > maxsplit) nsplit = (int)(maxsplit > minsplit ? maxsplit : minsplit);
+  if (nsplit < 1) nsplit = 1;
+  long long chunk = (maxrows + nsplit - 1) / nsplit;
+  chunk = (chunk + 31) / 32 * 32;
+  nsplit = (int)((maxrows + chunk - 1) / chunk);
+  if (nsplit < 1) nsplit = 1;
+  g.nsplit = nsplit;
+  long long off = 0;
+  for (int i = 0; i < ntask; ++i) {
+    g.t[i].part0 = off;
+    off += (long long)nsplit * g.t[i].ka * g.t[i].kb;
+  }
+  int rc = bdgd_ensure(c->stream, (void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
+  if (rc) return rc;
+  // oz_buf: the error flag (16 bytes), then the column maxima
+  const size_t mbytes = 16 + sizeof(unsigned long long) * (size_t)moff;
+  rc = bdgd_ensure(c->stream, &c->oz_buf, &c->oz_buf_bytes, mbytes);
+  if (rc) return rc;
+  unsigned long long *colmax = (unsigned long long *)((char *)c->oz_buf + 16);
+  g.colmax = colmax;
+  g.err = (int *)c->oz_buf;
+  g.part = c->gram_part;
+  BDGD_CK(cudaMemsetAsync(c->oz_buf, 0, mbytes, c->stream));
+  for (int i = 0; i < nops; ++i) {
+    const long long span = 65536;
+    const unsigned ny = (unsigned)((ops[i].rows + span - 1) / span);
+    bdgd_count_launch();
+    k_oz_colmax<<<dim3((unsigned)ops[i].k, ny ? ny : 1), 256, 0, c->stream>>>(ops[i].p, ops[i].ld, ops[i].rows, span,
+                                                                             colmax + ops[i].off);
+    BDGD_CK(cudaGetLastError());
+  }
+  if (!bdgd_capturing)
+    BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+  bdgd_count_launch();
+  k_gram_oz<<<(unsigned)(tiles * nsplit), OZ_THREADS, OZ_SMEM, c->stream>>>(g, chunk);
+  BDGD_CK(cudaGetLastError());
+  bdgd_count_launch();
+  k_oz_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, ldo, d_out);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+// the error flag of the last tensor-core Gram on this context (1: a wait on
+// the tensor core timed out); reads it synchronously
+extern "C" int bdgd_gram_oz_error(bdgd_ctx *c) {
+  if (!c->oz_buf || c->oz_buf_bytes < 16) return 0;
+  int h = 0;
+  if (cudaMemcpyAsync(&h, c->oz_buf, sizeof h, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return -1;
+  return h;
+}

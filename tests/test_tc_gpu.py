@@ -43,3 +43,94 @@ def test_i8_gemm_exact(bdg, M, N, K):
     assert int(err.item()) == 0
     ref = a.astype(np.int64) @ b.astype(np.int64).T
     assert np.array_equal(D.cpu().numpy().astype(np.int64), ref)
+
+
+def _gram_blocks(torch, rows, k, seed, kind):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    n = 2 * rows
+    X = torch.randn(k, n, dtype=torch.float64, device="cuda", generator=g)
+    if kind == "weighted":
+        # localised columns with a wide dynamic range (like psi0-weighted
+        # modes), a few tiny columns and one zero column
+        r = torch.linspace(-4, 4, n, dtype=torch.float64, device="cuda")
+        X = X * torch.exp(-0.5 * r * r)[None, :] * torch.logspace(0, -9, k, dtype=torch.float64, device="cuda")[:, None]
+        X[k // 2] = 0.0
+    AX = torch.randn(k, n, dtype=torch.float64, device="cuda", generator=g) * 1e3
+    return X, AX
+
+
+@pytest.mark.parametrize("rows,k,kind", [(4096, 64, "random"), (40000, 70, "weighted"), (262144, 192, "random"),
+                                         (131072, 130, "weighted")])
+def test_gram_tc_matches_reference(bdg, monkeypatch, rows, k, kind):
+    """The tensor-core FP64 Gram (int8 digits on tcgen05, exact int32 sums)
+    against the FP64 DMMA Gram and an extended-precision product: normwise
+    |G - G_ref| <= 1e-14 |a_i| |b_j| (the DMMA kernel is held to the same)."""
+    torch = _torch()
+    X, AX = _gram_blocks(torch, rows, k, rows + k, kind)
+    n = 2 * rows
+    dc = bdg.DeviceContext(3, [16, 16, 16], [8.0] * 3, False)
+    outs = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("BDG_GRAM_TC", mode)
+        out = torch.full((4 * k * k,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        dc.gram_ptr(0, False, rows, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr())
+        dc.synchronize()
+        outs[mode] = out.cpu().numpy().reshape(4, k, k)  # column-major k x k each: [j][i]
+    x = X.cpu().numpy().astype(np.longdouble)
+    ax = AX.cpu().numpy().astype(np.longdouble)
+    xu, xv = x[:, :rows], x[:, rows:]
+    ref = [xu @ xu.T, xv @ xv.T, xu @ xv.T, x @ ax.T]  # [i][j]
+    nu = np.sqrt(np.sum(xu * xu, axis=1))
+    nv = np.sqrt(np.sum(xv * xv, axis=1))
+    nx = np.sqrt(np.sum(x * x, axis=1))
+    na = np.sqrt(np.sum(ax * ax, axis=1))
+    scale = [np.outer(nu, nu), np.outer(nv, nv), np.outer(nu, nv), np.outer(nx, na)]
+    for mode, o in outs.items():
+        for q in range(4):
+            got = o[q].T  # [i][j]
+            sc = np.maximum(scale[q], 1e-300)
+            err = np.abs(got.astype(np.longdouble) - ref[q]) / sc
+            assert np.all(np.isfinite(got)), (mode, q)
+            assert float(err.max()) < 1e-14, (mode, q, float(err.max()))
+    dc.close()
+
+
+@pytest.mark.parametrize("fixture,nev", [("gs16", 4), ("c1_32", 8)])
+def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
+    """The whole solve with the tensor-core Gram: same eigenvalues as with the
+    DMMA Gram (1e-12 relative) and the true residual <= tol."""
+    import os
+
+    from oracle import bdg_oracle as O
+
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{fixture}.npz"))
+    N = [int(v) for v in f["N"]]
+    L = [float(v) for v in f["L"]]
+    om = [float(v) for v in f["omegas"]]
+    g, gdd, rc, mu, psi = float(f["g"]), float(f["gdd"]), float(f["rc"]), float(f["mu"]), f["psi"]
+    m, tol = 2 * nev, 1e-8
+    oc = O.Ctx(3, N, L)
+    X0 = O.gaussian_block_bpositive(oc, m, 0)
+    res = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("BDG_GRAM_TC", mode)
+        p = bdg.Problem(3, N, L)
+        p.set_system()
+        p.set_trap(O.harmonic_trap(oc, om))
+        p.set_wavefunction(psi)
+        p.set_local_interactions(lambda n: g * n, lambda n: g * n)
+        p.set_dipolar(gdd, [0.0, 0.0, 1.0], rc)
+        p.set_mu(mu)
+        p.set_solver_params(nev, m, 400, tol)
+        p.set_initial_block(X0)
+        p.set_goldstone_deflation(True)
+        p.set_convergence(bdg.CONV_TRUE_RESIDUAL)
+        assert p.solve() == 0 and p.converged() >= nev
+        st = p.stats()
+        assert st["max_true_residual"] <= tol
+        res[mode] = (p.eigenvalues()[:nev].copy(), st["iterations"])
+        p.close()
+    e0, e1 = res["0"][0], res["1"][0]
+    assert np.all(np.abs(e1 - e0) / np.abs(e0) < 1e-12), (e0, e1)
+    assert abs(res["1"][1] - res["0"][1]) <= 3
