@@ -1506,9 +1506,21 @@ static int launch_update(bdgd_ctx *c, const UArgs &u, long long nrt) {
   return BDGD_OK;
 }
 
+extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int nout, const bdgd_update_out *outs);
+
+// Tensor-core (int8 digits, tcgen05) FP64 update: on with BDG_UPDATE_TC=1
+static bool update_tc_on() {
+  const char *e = getenv("BDG_UPDATE_TC");
+  return e && e[0] == '1';
+}
+
 extern "C" int bdgd_block_update(bdgd_ctx *c, int prec, int cplx, uint64_t n, uint64_t ld, int nout,
                                  const bdgd_update_out *outs) {
   if (nout <= 0 || n == 0) return BDGD_OK;
+  if (prec == BDGD_F64 && !cplx && update_tc_on()) {
+    const int rc = bdgd_block_update_oz(c, n, ld, nout, outs);
+    if (rc != BDGD_ERR_UNSUPPORTED) return rc;
+  }
   if (prec != BDGD_F64 || cplx || nout > UMAXO || ld < n || (ld & 1)) return BDGD_ERR_UNSUPPORTED;
   UArgs u;
   memset(&u, 0, sizeof u);

@@ -557,3 +557,292 @@ extern "C" int bdgd_gram_oz_error(bdgd_ctx *c) {
     return -1;
   return h;
 }
+
+// ---------------------------------------------------------------------------
+// Basis update on the integer tensor cores: Y = alpha sum_b S_b C_b + beta Y
+// for real FP64 blocks (the interface of bdgd_block_update).  The same digit
+// scheme as the Gram with the roles turned: each ROW of S = [S_1 .. S_nt]
+// (over all its K = sum k_b columns) and each COLUMN of C are scaled by a
+// power of two from their maximum; 7 signed 8-bit digits each; diagonals
+// t + u >= 5 (34 MMAs per 32-wide K step) in 8 int32 TMEM accumulators.
+// A work unit is (output, 128-row tile, 64-column tile); C's digits for all K
+// steps stay in shared memory; S is read twice per unit (its row maxima,
+// then the digits), the second time from L2.
+// ---------------------------------------------------------------------------
+#define OZU_MAXK 256                   // K = sum k_b limit (8 steps of 32)
+#define OZU_SMEM_C (8 * OZ_ND * 64 * 32)  // C digits of up to 8 K steps
+#define OZU_SMEM_A (2 * OZ_ND * 128 * 32) // two stages of S digits
+#define OZU_SMEM (OZU_SMEM_C + OZU_SMEM_A + 4096)
+
+struct OzuTerm {
+  const double *s, *c;
+  int k, ldc, nst;  // columns, C leading dim, K steps of 32
+};
+struct OzuOut {
+  double *y;
+  int ncol, nterm;
+  double alpha, beta;
+  OzuTerm t[3];
+  int nst;          // K steps over all terms
+};
+struct OzuArgs {
+  OzuOut o[4];
+  int nout;
+  int ct_out[64], ct_col[64], nct;  // (output, 64-column tile) pairs
+  long long n, ld, nrt;
+  int *err;
+};
+
+// 16 values of row r: columns [j0, j0 + 16) of term tm (zero past k or n)
+__device__ __forceinline__ void ozu_load_row16(const OzuTerm &tm, long long ld, long long r, long long n, int j0,
+                                               double (&v)[16]) {
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int j = j0 + q;
+    v[q] = (r < n && j < tm.k) ? __ldg(tm.s + (long long)j * ld + r) : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
+  extern __shared__ __align__(1024) uint8_t oz_smem[];
+  uint8_t *cdig = oz_smem;                        // [step][digit][64 x 32]
+  uint8_t *adig = oz_smem + OZU_SMEM_C;           // [stage][digit][128 x 32]
+  double *rmax = reinterpret_cast<double *>(oz_smem + OZU_SMEM_C + OZU_SMEM_A);  // [2][128]
+  double *cmax = rmax + 256;                                                  // [2][64]
+  int *cexpo = reinterpret_cast<int *>(cmax + 128);                           // [64] column exponents
+  int *cbadf = cexpo + 64;                                                    // [64] non-finite columns
+  uint64_t *bar = reinterpret_cast<uint64_t *>(cbadf + 64);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long unit = blockIdx.x;
+  const int ct = (int)(unit % u.nct);
+  const long long rt = unit / u.nct;
+  const OzuOut &o = u.o[u.ct_out[ct]];
+  const int c0 = 64 * u.ct_col[ct];
+  const long long r0 = rt * 128;
+  const long long n = u.n, ld = u.ld;
+
+  if (warp == 0) tmem_alloc(tslot, 512);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  // C: column maxima over all K, then the digits of every K step
+  const int cc = tid & 63, ch = (tid >> 6) & 1;  // threads < 128
+  {
+    double m = 0.0;
+    if (tid < 128 && c0 + cc < o.ncol) {
+      for (int b = 0; b < o.nterm; ++b) {
+        const OzuTerm &tm = o.t[b];
+        const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
+        for (int j = ch; j < tm.k; j += 2) {
+          const double x = fabs(col[j]);
+          m = (x > m || x != x) ? x : m;
+        }
+      }
+    }
+    if (tid < 128) cmax[ch * 64 + cc] = m;
+  }
+  // S: row maxima over all K
+  const int rr = tid & 127, rh = tid >> 7;
+  {
+    double m = 0.0;
+    const long long r = r0 + rr;
+    if (r < n)
+      for (int b = 0; b < o.nterm; ++b) {
+        const OzuTerm &tm = o.t[b];
+        for (int j = rh; j < tm.k; j += 2) {
+          const double x = fabs(__ldg(tm.s + (long long)j * ld + r));
+          m = (x > m || x != x) ? x : m;
+        }
+      }
+    rmax[rh * 128 + rr] = m;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  // scales
+  double cs = 1.0, rs = 1.0;
+  int cS = 0, rS = 0;
+  bool cbad = false, rbad = false;
+  {
+    const double m0 = cmax[cc], m1 = cmax[64 + cc];
+    const double mc = (m0 > m1 || m0 != m0) ? m0 : m1;
+    bool fin = true;
+    oz_scale((unsigned long long)__double_as_longlong(mc), cs, cS, fin);
+    cbad = !fin;
+    const double n0 = rmax[rr], n1 = rmax[128 + rr];
+    const double mr = (n0 > n1 || n0 != n0) ? n0 : n1;
+    oz_scale((unsigned long long)__double_as_longlong(mr), rs, rS, fin);
+    rbad = !fin;
+    if (tid < 64) {
+      cexpo[cc] = cS;
+      cbadf[cc] = cbad;
+    }
+  }
+  // C digits: thread (cc, ch) writes K rows [16 ch, 16 ch + 16) of every step
+  if (tid < 128) {
+    int step = 0;
+    for (int b = 0; b < o.nterm; ++b) {
+      const OzuTerm &tm = o.t[b];
+      const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
+      const bool vc = c0 + cc < o.ncol;
+      for (int s = 0; s < tm.nst; ++s, ++step) {
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int j = 32 * s + 16 * ch + q;
+          v[q] = (vc && j < tm.k) ? col[j] : 0.0;
+        }
+        uint4 d[OZ_ND];
+        oz_digits16(v, cs, d);
+        const int off = (cc & 7) * 16 + (cc >> 3) * 256 + ch * 128;
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t)
+          *reinterpret_cast<uint4 *>(cdig + (step * OZ_ND + t) * 2048 + off) = d[t];
+      }
+    }
+  }
+  // main loop over K steps: S digits (row rr, K columns [16 rh, 16 rh + 16))
+  const int offA = (rr & 7) * 16 + (rr >> 3) * 256 + rh * 128;
+  uint32_t ph[2] = {0u, 0u};
+  int failed = 0;
+  int step = 0;
+  for (int b = 0; b < o.nterm && !failed; ++b) {
+    const OzuTerm &tm = o.t[b];
+    for (int s = 0; s < tm.nst; ++s, ++step) {
+      const int st = step & 1;
+      double v[16];
+      ozu_load_row16(tm, ld, r0 + rr, n, 32 * s + 16 * rh, v);
+      uint4 d[OZ_ND];
+      oz_digits16(v, rs, d);
+      if (step >= 2) {
+        const bool ok = mbar_wait(&bar[st], ph[st], TC_WAIT_LIMIT);
+        ph[st] ^= 1u;
+        failed = __syncthreads_or(!ok);
+        if (failed) break;
+      }
+      uint8_t *sa = adig + st * (OZ_ND * 4096);
+#pragma unroll
+      for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(sa + t * 4096 + offA) = d[t];
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t id = idesc_i8(64);
+        const uint32_t abase = smem_u32(sa), bbase = smem_u32(cdig + step * OZ_ND * 2048);
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t)
+#pragma unroll
+          for (int q = 0; q < OZ_ND; ++q) {
+            const int D = t + q;
+            if (D < OZ_DMIN) continue;
+            const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+            mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(abase + t * 4096), smem_desc(bbase + q * 2048),
+                   id, (step > 0 || t > first_t) ? 1u : 0u);
+          }
+        mma_commit(&bar[st]);
+      }
+    }
+  }
+  const int nsteps = step;
+  if (!failed && nsteps > 0) {
+    const int st = (nsteps - 1) & 1;
+    const bool ok = mbar_wait(&bar[st], ph[st], TC_WAIT_LIMIT);
+    failed = __syncthreads_or(!ok);
+  }
+  tc_fence_after();
+  if (failed) {
+    if (tid == 0) atomicExch(u.err, 1);
+  } else if (nsteps > 0) {
+    // flush: warp w has TMEM lanes (rows) 32 (w % 4).., output columns 32 (w / 4)..
+    const int row = 32 * (warp & 3) + lane;
+    const long long r = r0 + row;
+    // this thread's own row scale is row's: rr = tid & 127 = 32 (warp % 4) + lane
+    for (int grp = 0; grp < 2; ++grp) {
+      const int cl = 32 * (warp >> 2) + 16 * grp;
+      double acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+#pragma unroll
+      for (int d = 0; d < OZ_NDIAG; ++d) {
+        int32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + cl), v);
+        const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
+      }
+      if (r < n) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int c = c0 + cl + q;
+          if (c < o.ncol) {
+            double val = o.alpha * ldexp(acc[q], rS + cexpo[cl + q]);
+            if (rbad || cbadf[cl + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+            double *yp = o.y + (long long)c * ld + r;
+            if (o.beta != 0.0) val += o.beta * *yp;
+            *yp = val;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 512);
+}
+
+// Real FP64 block update on the tensor cores (bdgd_block_update's interface);
+// BDGD_ERR_UNSUPPORTED (nothing launched) outside its limits.
+extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int nout, const bdgd_update_out *outs) {
+  if (nout <= 0 || n == 0) return BDGD_OK;
+  if (nout > 4 || ld < n) return BDGD_ERR_UNSUPPORTED;
+  OzuArgs u;
+  memset(&u, 0, sizeof u);
+  u.n = (long long)n;
+  u.ld = (long long)ld;
+  u.nout = nout;
+  for (int i = 0; i < nout; ++i) {
+    const bdgd_update_out &s = outs[i];
+    if (s.nterm < 0 || s.nterm > 3 || s.ncol < 0 || ((uintptr_t)s.y % 8)) return BDGD_ERR_UNSUPPORTED;
+    OzuOut &o = u.o[i];
+    o.y = (double *)s.y;
+    o.ncol = s.ncol;
+    o.alpha = s.alpha;
+    o.beta = s.beta;
+    int ktot = 0;
+    for (int b = 0; b < s.nterm; ++b) {
+      if (s.term[b].k <= 0) continue;
+      if (((uintptr_t)s.term[b].s % 8) || s.term[b].ldc < s.term[b].k || ((uintptr_t)s.term[b].c % 8))
+        return BDGD_ERR_UNSUPPORTED;
+      OzuTerm &t = o.t[o.nterm++];
+      t.s = (const double *)s.term[b].s;
+      t.c = s.term[b].c;
+      t.k = s.term[b].k;
+      t.ldc = s.term[b].ldc;
+      t.nst = (t.k + 31) / 32;
+      o.nst += t.nst;
+      ktot += t.k;
+    }
+    if (o.nst > 8 || ktot > OZU_MAXK) return BDGD_ERR_UNSUPPORTED;
+    for (int j = 0; o.nterm > 0 && j * 64 < s.ncol; ++j) {  // no terms: Y untouched
+      if (u.nct == 64) return BDGD_ERR_UNSUPPORTED;
+      u.ct_out[u.nct] = i;
+      u.ct_col[u.nct] = j;
+      u.nct++;
+    }
+  }
+  if (u.nct == 0) return BDGD_OK;
+  u.nrt = ((long long)n + 127) / 128;
+  int rc = bdgd_ensure(c->stream, &c->oz_buf, &c->oz_buf_bytes, 16);
+  if (rc) return rc;
+  u.err = (int *)c->oz_buf;
+  if (!bdgd_capturing)
+    BDGD_CK(cudaFuncSetAttribute(k_update_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZU_SMEM));
+  bdgd_count_launch();
+  k_update_oz<<<(unsigned)(u.nrt * u.nct), OZ_THREADS, OZU_SMEM, c->stream>>>(u);
+  return bdgd_check(cudaGetLastError(), "k_update_oz");
+}

@@ -98,8 +98,8 @@ def test_gram_tc_matches_reference(bdg, monkeypatch, rows, k, kind):
 
 @pytest.mark.parametrize("fixture,nev", [("gs16", 4), ("c1_32", 8)])
 def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
-    """The whole solve with the tensor-core Gram: same eigenvalues as with the
-    DMMA Gram (1e-12 relative) and the true residual <= tol."""
+    """The whole solve with the tensor-core Gram and update: same eigenvalues
+    as with the DMMA kernels (1e-12 relative) and the true residual <= tol."""
     import os
 
     from oracle import bdg_oracle as O
@@ -115,6 +115,7 @@ def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
     res = {}
     for mode in ("0", "1"):
         monkeypatch.setenv("BDG_GRAM_TC", mode)
+        monkeypatch.setenv("BDG_UPDATE_TC", mode)
         p = bdg.Problem(3, N, L)
         p.set_system()
         p.set_trap(O.harmonic_trap(oc, om))
@@ -134,3 +135,50 @@ def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
     e0, e1 = res["0"][0], res["1"][0]
     assert np.all(np.abs(e1 - e0) / np.abs(e0) < 1e-12), (e0, e1)
     assert abs(res["1"][1] - res["0"][1]) <= 3
+
+
+@pytest.mark.parametrize("n,m,beta", [(8192, 16, 0.0), (100000, 64, 0.0), (65536, 40, 1.0)])
+def test_update_tc_matches_reference(bdg, monkeypatch, n, m, beta):
+    """The tensor-core FP64 basis update Y = alpha sum_b S_b C_b + beta Y
+    (the iteration's X' = [X P W] Cx, P' = [P W] Cp and a beta = 1
+    projection shape) against the DMMA update and an extended-precision
+    product: normwise |Y - Y_ref| <= 1e-14 (|S_r| |C_c| + |beta Y|)."""
+    torch = _torch()
+    g = torch.Generator(device="cuda").manual_seed(n + m)
+    blk = {nm: torch.randn(m, n, dtype=torch.float64, device="cuda", generator=g) for nm in ("X", "P", "W")}
+    r = torch.linspace(-3, 3, n, dtype=torch.float64, device="cuda")
+    blk["W"] = blk["W"] * torch.exp(-r * r)[None, :] * 1e-6  # small, localised search directions
+    Cx = torch.randn(m, 3 * m, dtype=torch.float64, device="cuda", generator=g)  # (3m x m) column-major
+    Cp = torch.randn(m, 2 * m, dtype=torch.float64, device="cuda", generator=g)
+    Y0 = torch.randn(m, n, dtype=torch.float64, device="cuda", generator=g)
+    e8 = 8
+
+    def terms(names, Cm):
+        return [(blk[nm].data_ptr(), m, Cm.data_ptr() + i * m * e8, Cm.shape[1]) for i, nm in enumerate(names)]
+
+    results = {}
+    dc = bdg.DeviceContext(3, [16, 16, 16], [8.0] * 3, False)
+    for mode in ("0", "1"):
+        monkeypatch.setenv("BDG_UPDATE_TC", mode)
+        ys = [Y0.clone(), Y0.clone()]
+        outs = [(ys[0].data_ptr(), m, 1.0, beta, terms(("X", "P", "W"), Cx)),
+                (ys[1].data_ptr(), m, -1.0, beta, terms(("P", "W"), Cp))]
+        torch.cuda.synchronize()
+        assert dc.block_update(0, False, n, n, outs) == 0
+        dc.synchronize()
+        results[mode] = [y.cpu().numpy() for y in ys]
+    S = {k: v.cpu().numpy().astype(np.longdouble) for k, v in blk.items()}
+    cx = Cx.cpu().numpy().astype(np.longdouble)  # [col][k]
+    cp = Cp.cpu().numpy().astype(np.longdouble)
+    y0 = Y0.cpu().numpy().astype(np.longdouble)
+    Sx = np.concatenate([S["X"], S["P"], S["W"]])  # (3m, n)
+    Sp = np.concatenate([S["P"], S["W"]])
+    refs = [cx @ Sx + beta * y0, -(cp @ Sp) + beta * y0]
+    scales = [np.outer(np.sqrt((cx * cx).sum(1)), np.sqrt((Sx * Sx).sum(0))) + abs(beta) * np.abs(y0),
+              np.outer(np.sqrt((cp * cp).sum(1)), np.sqrt((Sp * Sp).sum(0))) + abs(beta) * np.abs(y0)]
+    for mode, ys in results.items():
+        for q in range(2):
+            err = np.abs(ys[q].astype(np.longdouble) - refs[q]) / np.maximum(scales[q], 1e-300)
+            assert np.all(np.isfinite(ys[q])), (mode, q)
+            assert float(err.max()) < 1e-14, (mode, q, float(err.max()))
+    dc.close()
