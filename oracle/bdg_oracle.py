@@ -19,7 +19,8 @@ relative to that project's root):
 * preconditioner T_K, T_M, T_Lrep   src/precond_impl.inc:21-118
 * dipolar kernel / mean field  src/dipolar.c:21-72, src/dipolar_meanfield_impl.inc:20-55
 * setup (trap grid, interactions, mu, precond sqrt)   src/setup.c:17-197
-* init modes (planewave, wf-weighted, reuse)          src/solver.c:68-259, src/bdg.c:112-207
+* init modes: PLANEWAVE (real and complex), complex WF_WEIGHTED
+                                                      src/solver.c:68-259, :321-414
 
 FFTs follow FFTW's conventions as the reference uses them: unnormalised
 transforms, dims reversed so x is fastest, r2c halving the x axis
@@ -33,10 +34,14 @@ Numer. Algorithms 66 (2014) -- block trace minimisation of x^T A x / x^T B x
 over B-positive subspaces, Rayleigh-Ritz on span[X, T R, P].  The GPU solver
 in the product runs the same iteration; see ``ilobpcg`` below.
 
-Parity pinning: the operator restatement is checked against every known-answer
-value in the reference's own tests (tests/golden/reference_known_answers.json,
-transcribed from tests/test_*.c) and, when it has been built, against the
-reference's own C sources compiled under oracle/_ref.
+Parity pinning (tests/test_ref_oracle_cpu.py, tests/test_oracle_cpu.py):
+* against the reference's own C sources, compiled unmodified into
+  oracle/_ref (oracle/Makefile): setup fields and all nine operators to
+  1e-13 on the 32^3 benchmark trap (real and complex psi0), the init-mode
+  blocks bit for bit (real) or to the rounding of cabs (complex), and the
+  solve of the reference's own solve path on the same inputs;
+* the reference's own tests/test_*.c, run against that build;
+* the known-answer assertions of those tests, restated in tests/cases.py.
 """
 from __future__ import annotations
 
@@ -800,8 +805,12 @@ def itp_ground_state(N, L, omegas, g, gdd=0.0, dipole_dir=(0.0, 0.0, 1.0),
         n = np.abs(p) ** 2
         U = V + g * n
         if vdd is not None:
-            phi = sfft.irfftn(sfft.rfftn(n, workers=_WORKERS) * vdd, s=ctx.rshape,
-                              norm="forward", workers=_WORKERS)
+            if vortex:  # the kernel is on the full spectrum of the complex context
+                phi = np.real(sfft.ifftn(sfft.fftn(n, workers=_WORKERS) * vdd, norm="forward",
+                                         workers=_WORKERS))
+            else:
+                phi = sfft.irfftn(sfft.rfftn(n, workers=_WORKERS) * vdd, s=ctx.rshape,
+                                  norm="forward", workers=_WORKERS)
             U = U + gdd * phi
         return U
 
