@@ -1091,6 +1091,22 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   return 0;
 }
 
+/* A REUSE block (modes of the previous solve plus noise) is not always
+ * B-positive: with an undeflated zero mode among the reused modes (u large,
+ * v near zero) the B-form of the block is indefinite and the Rayleigh-Ritz
+ * step finds fewer than sizeSub positive-type directions.  The solve then
+ * goes on from a fresh B-positive block (WF_WEIGHTED, u = v) instead of
+ * failing, as the reference's bdg_solve goes on (it returns 0 always,
+ * src/solver.c:285). */
+static int restart_b_positive(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, double *lam, double *res,
+                              uint64_t *iters, int *nconv) {
+  fprintf(stderr, "bdg_solve: the REUSE block is not B-positive; starting from WF_WEIGHTED instead\n");
+  bdg->init_mode = BDG_INIT_WF_WEIGHTED;
+  const int rc = bdg_fill_initial_block_device(bdg, w->blk[NB_X], w->prec);
+  if (rc != 0) return rc < 0 ? rc : -5;
+  return run_loop(w, dev, bdg, o, lam, res, iters, nconv, 0);
+}
+
 /* hand the FP32 phase's X and P blocks to the FP64 workspace */
 static int to_f64(ws_t *w32, ws_t *w64, bdgd_ctx *dev) {
   const uint64_t es = w32->cplx ? 2 : 1;
@@ -1133,6 +1149,9 @@ static int solve_gpu(bdg_t *bdg) {
    * fill and upload (converted for FP32) for CUSTOM and a stored REUSE
    * buffer, or with BDG_HOST_INIT=1 */
   int host_init = 1;
+  /* a stored REUSE buffer of the right shape is the start (bdg_reuse_modes) */
+  const int from_reuse = bdg->init_mode == BDG_INIT_REUSE && bdg->reuse_buf && bdg->reuse_n == n &&
+                         bdg->reuse_cols == m;
   if (!getenv("BDG_HOST_INIT")) {
     host_init = bdg_fill_initial_block_device(bdg, w->blk[NB_X], w->prec);
     if (host_init < 0) {
@@ -1210,6 +1229,7 @@ static int solve_gpu(bdg_t *bdg) {
     o32.stop_backward_at_floor = 1;
     o32.floor = sw_at;
     rc = run_loop(w, dev, bdg, &o32, lam, res, &iters, &nconv, 0);
+    if (rc == -5 && from_reuse) rc = restart_b_positive(w, dev, bdg, &o32, lam, res, &iters, &nconv);
     if (!rc) {
       ws_t *w64 = &wsp[0];
       if ((rc = ws_setup(w64, dev, S, m, nev, cplx, BDGD_F64))) return rc;
@@ -1223,6 +1243,7 @@ static int solve_gpu(bdg_t *bdg) {
     }
   } else {
     rc = run_loop(w, dev, bdg, &o, lam, res, &iters, &nconv, 0);
+    if (rc == -5 && from_reuse) rc = restart_b_positive(w, dev, bdg, &o, lam, res, &iters, &nconv);
   }
   cudaEventRecord(e1, st);
   cudaEventSynchronize(e1);

@@ -186,3 +186,30 @@ def test_goldstone_deflation_complex_psi0(bdg):
             assert np.all(np.abs(ev[-1] - ref.eigvals[:4]) / ref.eigvals[:4] < 1e-9)
         p.close()
     assert np.all(np.abs(ev[0] - ev[1]) / ev[0] < 1e-9)
+
+
+def test_reuse_sweep_with_undeflated_zero_mode(bdg):
+    """tests/test_io.c:390-446 (sweep_reuse_1d) of the reference: a 1D uniform
+    gas, nev 2 / sizeSub 5 with the Goldstone mode among the wanted pairs,
+    bdg_reuse_modes, reset, mu * 1.01, solve again.  The reused block is not
+    B-positive (the zero mode has u large, v near zero); the second solve goes
+    on from a fresh B-positive block and returns 0 with eigenvalues, as the
+    reference's bdg_solve does."""
+    p = bdg.Problem(1, [32], [10.0])
+    p.set_system()
+    p.set_solver_params(2, 5, 200, 1e-5)
+    wf = np.ones(32)
+    p.set_wavefunction(wf)
+    p.set_local_interactions(lambda n: 1.0 * n, lambda n: 1.0 * n)
+    p.set_mu(1.0)
+    assert p.solve() == 0
+    ev1 = p.eigenvalues().copy()
+    assert p.reuse_modes(0.01) == 0
+    p._L.bdg_reset(p._h)
+    p.set_wavefunction(wf)
+    p.set_local_interactions(lambda n: 1.0 * n, lambda n: 1.0 * n)
+    p.set_mu(1.01)
+    assert p.solve() == 0
+    ev2 = p.eigenvalues()
+    assert ev2 is not None and np.all(np.isfinite(ev2)) and len(ev2) == 2 and len(ev1) == 2
+    p.close()
