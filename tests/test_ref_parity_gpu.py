@@ -231,3 +231,35 @@ def test_c1_solve_matches_reference_solve(bdg, c1_reference_solve, precision):
     v = p.modes_v()
     assert _angles(v[:7], r["v"][:7]) <= 1e-6
     p.close()
+
+
+def test_c1_complex_solve_matches_reference_solve(bdg):
+    """The complex (_z) path: psi0 = e^{0.7 i} x the stationary 32^3 state (a
+    genuinely complex condensate with the real problem's spectrum), complex
+    N(0,1) block with v = u at seed 2, true residual <= 1e-8, Goldstone chain
+    deflated; GPU against the reference's complex solve path (z_ilobpcg of
+    the oracle build): eigenvalues 1e-9, true residual <= tol, and the same
+    eigenvalues as the real problem."""
+    N, L, om, g, gdd, rc, mu, psi = _fixture("c1_32")
+    psi_z = psi * np.exp(0.7j)
+    nev, m, tol = 8, 16, 1e-8
+    oc = O.Ctx(3, N, L, True)
+    X0 = O.gaussian_block_bpositive(oc, m, 2)
+    rp = R.build_problem(N, L, om, g, gdd, psi_z, mu, Rc=rc, complex_psi0=True)
+    rp.set_solver_params(nev, m, 400, tol)
+    rp.set_initial_block(X0)
+    ref = rp.solve(criterion=R.CONV_TRUE_RESIDUAL, deflate=True)
+    rp.close()
+    assert ref["converged"] >= nev
+    p = _product_problem(bdg, N, L, om, g, gdd, rc, mu, psi_z, cplx=True)
+    p.set_solver_params(nev, m, 400, tol)
+    p.set_initial_block(X0)
+    p.set_goldstone_deflation(True)
+    p.set_convergence(bdg.CONV_TRUE_RESIDUAL)
+    assert p.solve() == 0 and p.converged() >= nev
+    ev = p.eigenvalues()[:nev]
+    assert np.all(np.abs(ev - ref["eigvals"]) / np.abs(ref["eigvals"]) < 1e-9), (ev, ref["eigvals"])
+    assert p.stats()["max_true_residual"] <= tol
+    real = np.load(os.path.join(HERE, "golden", "c1_32_solve.npz"))["eigvals"][:nev]
+    assert np.all(np.abs(ev - real) / real < 1e-9)
+    p.close()
