@@ -13,6 +13,7 @@
  *   repeat:  norms of R = AX - B X diag(lam) (swap folded into the kernel)
  *            test the nev wanted pairs; active set = unconverged columns
  *            W = T R_active                     (batched FFT operator kernels)
+ *            P <- P - X (X^H X)^+ X^H P, SVQB   (AP transformed alike)
  *            W <- W - Q (Q^H Q)^+ Q^H W, SVQB   (Q = [X, P]),  AW = A W
  *            Rayleigh-Ritz on S = [X, P, W] from the Gram blocks
  *              S^H S, S^H A S, S_u^H S_v (FP64 tensor-core contraction;
@@ -990,17 +991,40 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
     }
     cudaEventRecord(w->ev[5], st);
     TRY(deflate_block(w, dev, B(NB_WT), na));
-    /* P enters Q = [X, P] as the last update left it: no explicit projection
-     * of P against X and no SVQB of P (the W projection against [X, P] and
-     * the implicit orthonormalisation of the Rayleigh-Ritz step keep the
-     * basis conditioned; same eigenvalues in equal or fewer iterations) */
-    const int pk = w->p;
+    const int p = w->p;
+    /* P <- (P - X (X^H X)^+ X^H P) Z_P ; AP alike */
+    int pk = 0;
+    if (p > 0) {
+      bdgd_gram_task t[2];
+      t[0] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0);
+      t[1] = mk_task(w, B(NB_X), B(NB_P), w->n, m, p, 0, 0, m, 0, 0);
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 2, t, K, w->gout));
+      TRY(gram_pinv_apply(w, dev, w->gout, m, K, w->gout + (size_t)m * K * es, p, drop, w->Cs));
+      {
+        bdgd_update_out o[2] = {upd_out(B(NB_P), p, -1.0, 1.0), upd_out(B(NB_AP), p, -1.0, 1.0)};
+        upd_term(&o[0], B(NB_X), m, w->Cs, m);
+        upd_term(&o[1], B(NB_AX), m, w->Cs, m);
+        TRY(bupdate(w, dev, 0, 2, o));
+      }
+      t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 1, 0, 0, 1, 0);
+      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
+      TRY(svqb(w, dev, w->gout + (size_t)K * K * es, p, K, drop, w->Cs, &pk));
+      /* Cs holds Z_P (p x pk, leading dim p) */
+      {
+        bdgd_update_out o[2] = {upd_out(B(NB_T1), pk, 1.0, 0.0), upd_out(B(NB_T2), pk, 1.0, 0.0)};
+        upd_term(&o[0], B(NB_P), p, w->Cs, p);
+        upd_term(&o[1], B(NB_AP), p, w->Cs, p);
+        TRY(bupdate(w, dev, 0, 2, o));
+      }
+      swapb(w, NB_P, NB_T1);
+      swapb(w, NB_AP, NB_T2);
+    }
     /* W <- (Wt - Q (Q^H Q)^+ Q^H Wt) Z_W, Q = [X, P] */
     const int q = m + pk;
     {
       bdgd_gram_task t[5];
       int nt = 0;
-      t[nt++] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0);
+      if (p == 0) t[nt++] = mk_task(w, B(NB_X), B(NB_X), w->n, m, m, 0, 0, 0, 1, 0); /* else kept from above */
       t[nt++] = mk_task(w, B(NB_X), B(NB_WT), w->n, m, na, 0, 0, q, 0, 0);
       if (pk > 0) {
         t[nt++] = mk_task(w, B(NB_X), B(NB_P), w->n, m, pk, 0, 0, m, 0, 1);

@@ -109,7 +109,8 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
   bdgd_count_launch();
   k_tc_i8_gemm<<<dim3((unsigned)(M / 128), (unsigned)(N / 64)), 128, 0, (cudaStream_t)stream>>>(
       A, (long long)lda, B, (long long)ldb, D, (long long)ldd, (int)K, d_err);
-  return bdgd_check(cudaGetLastError(), "k_tc_i8_gemm");
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -844,5 +845,6 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
     BDGD_CK(cudaFuncSetAttribute(k_update_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZU_SMEM));
   bdgd_count_launch();
   k_update_oz<<<(unsigned)(u.nrt * u.nct), OZ_THREADS, OZU_SMEM, c->stream>>>(u);
-  return bdgd_check(cudaGetLastError(), "k_update_oz");
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
 }
