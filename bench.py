@@ -127,16 +127,21 @@ def cpu_model():
     return "unknown"
 
 
-def cached_solve(grid):
+def cached_solve(grid, mu=None):
     """The full FP64 reference-path solve of this configuration, run once on
-    the host (tests/golden/make_fixtures.py solve): eigenvalues, iterations
-    to tolerance and its per-iteration wall clock."""
+    the host (tests/golden/make_fixtures.py solve / solve_config):
+    eigenvalues, iterations to tolerance and its per-iteration wall clock.
+    None if absent, or if it was made from a psi0 whose mu differs from this
+    run's (relative 1e-10)."""
     name = {32: "c1_32", 64: "c2_64", 128: "c2_128"}.get(grid)
     path = os.path.join(ROOT, "tests", "golden", f"{name}_solve.npz") if name else None
     if not path or not os.path.exists(path):
         return None
     d = np.load(path)
-    return {k: d[k] for k in d.files}
+    out = {k: d[k] for k in d.files}
+    if mu is not None and "mu" in out and abs(float(out["mu"]) - mu) > 1e-10 * abs(mu):
+        return None
+    return out
 
 
 def reference_solve_sample(cfg, psi, mu, V, X0, iters, threads):
@@ -216,7 +221,7 @@ def run_reference(args, cfg):
         return 0
     psi, mu, V, X0 = inp
     threads = os.cpu_count() or 1
-    cached = cached_solve(N[0])
+    cached = cached_solve(N[0], mu)
     t0 = time.perf_counter()
     tl, res = reference_solve_sample(cfg, psi, mu, V, X0, args.warmup + args.steps, threads)
     wall = time.perf_counter() - t0
@@ -666,7 +671,7 @@ def main():
         "gpu_launches": int(launches),
         "clocks": ck,
     }
-    cached = cached_solve(cfg["N"][0])
+    cached = cached_solve(cfg["N"][0], mu)
     ce = None
     if cached is not None:
         # per-eigenvalue relative error against the FP64 CPU oracle solve of the same input

@@ -12,6 +12,7 @@ K psi0 = 0 to ~1e-14 and the Goldstone mode is exact.
 
     python tests/golden/make_fixtures.py [name ...]
     python tests/golden/make_fixtures.py solve <name> <nev> <seed> [threads]
+    python tests/golden/make_fixtures.py solve_config <grid> <psi.npz> [threads]
 """
 import os
 
@@ -81,6 +82,38 @@ def solve(name, nev, seed, threads=None):
     print(res["eigvals"])
 
 
+def solve_config(grid, psi_file, threads=None):
+    """The FP64 reference-path solve of the benchmark configuration at
+    `grid`^3 (bdg_lobpcg_b200.problems.config) from the psi0 in `psi_file`
+    (an .npz with psi and mu from the library's GPU ground-state producer,
+    the same psi0 the benchmark computes): writes c2_<grid>_solve.npz with
+    the eigenvalues, iterations to tolerance, per-iteration wall clock and the
+    psi0's mu and norms, by which bench.py recognises its input."""
+    from bdg_lobpcg_b200 import problems
+    from oracle import ref as R
+
+    cfg = problems.config(grid)
+    d = np.load(psi_file)
+    psi, mu = d["psi"], float(d["mu"])
+    threads = threads or os.cpu_count() or 1
+    R.set_threads(threads)
+    V = problems.trap(cfg["N"], cfg["L"], cfg["omegas"])
+    rp = R.build_problem(cfg["N"], cfg["L"], cfg["omegas"], cfg["g"], cfg["gdd"], psi, mu, V=V, Rc=cfg["rc"])
+    size = int(np.prod(cfg["N"]))
+    u = np.random.default_rng(cfg["seed"]).standard_normal((cfg["sizeSub"], size))
+    rp.set_solver_params(cfg["nev"], cfg["sizeSub"], 2000, cfg["tol"])
+    rp.set_initial_block(np.concatenate([u, u], axis=1))
+    t = time.time()
+    res = rp.solve(criterion=R.CONV_TRUE_RESIDUAL, deflate=True)
+    np.savez_compressed(os.path.join(HERE, f"c2_{grid}_solve.npz"), eigvals=res["eigvals"],
+                        iterations=res["iterations"], converged=res["converged"], timeline=res["timeline"],
+                        nev=cfg["nev"], sizeSub=cfg["sizeSub"], seed=cfg["seed"], threads=threads, mu=mu,
+                        psi_l1=float(np.sum(np.abs(psi))), psi_max=float(np.max(np.abs(psi))))
+    print(grid, "solve", res["iterations"], "iterations", res["converged"], "converged",
+          "%.1fs" % (time.time() - t))
+    print(res["eigvals"])
+
+
 def load(name):
     d = np.load(os.path.join(HERE, f"{name}.npz"))
     return {k: d[k] for k in d.files}
@@ -91,6 +124,9 @@ if __name__ == "__main__":
     if args[:1] == ["solve"]:
         # python tests/golden/make_fixtures.py solve c2_64 16 1 [threads]
         solve(args[1], int(args[2]), int(args[3]), int(args[4]) if len(args) > 4 else None)
+    elif args[:1] == ["solve_config"]:
+        # python tests/golden/make_fixtures.py solve_config 128 psi_128.npz [threads]
+        solve_config(int(args[1]), args[2], int(args[3]) if len(args) > 3 else None)
     else:
         for nm in (args or list(PROBLEMS)):
             make(nm)
