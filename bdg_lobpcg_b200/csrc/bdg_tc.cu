@@ -227,144 +227,213 @@ __device__ __forceinline__ void oz_load16(const double *__restrict__ col, long l
   }
 }
 
-__global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk) {
+// bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to this CTA's shared memory, completing on the mbarrier's tx count
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Raw FP64 stage: 32 rows of each of the tile's columns, column c at
+// c * OZ_RAW_LD bytes (272: 16-byte aligned for the bulk copies, and 68 words
+// apart so that 8 consecutive columns fall in 8 different bank groups).
+#define OZ_RAW_LD 272
+#define OZ_RAW_A (128 * OZ_RAW_LD)
+#define OZ_RAW_STAGE (OZ_RAW_A + 64 * OZ_RAW_LD)
+#define OZ_SMEM2 (2 * OZ_RAW_STAGE + 2 * OZ_STAGE + 4096)
+
+// issue the bulk copies of step `ks` of the unit into raw stage `st` (warp 0)
+__device__ __forceinline__ void oz_issue_step(const OzTask &tk, int ia, int jb, long long r, uint8_t *raw,
+                                              uint64_t *full, int lane) {
+  const int na = min(128, tk.ka - ia * 128), nb = min(64, tk.kb - jb * 64);
+  if (lane == 0) mbar_expect_tx(full, (uint32_t)(na + nb) * 256u);
+  __syncwarp();
+  for (int c = lane; c < na; c += 32)
+    bulk_g2s(raw + c * OZ_RAW_LD, tk.a + (long long)(ia * 128 + c) * tk.lda + r, 256u, full);
+  for (int c = lane; c < nb; c += 32)
+    bulk_g2s(raw + OZ_RAW_A + c * OZ_RAW_LD, tk.b + (long long)(jb * 64 + c) * tk.ldb + r, 256u, full);
+}
+
+// 16 doubles (rows 16 h .. 16 h + 15) of column c of a raw stage region
+__device__ __forceinline__ void oz_raw16(const uint8_t *region, int c, int h, bool valid, double (&v)[16]) {
+  if (valid) {
+    const double2 *p = reinterpret_cast<const double2 *>(region + c * OZ_RAW_LD + h * 128);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double2 x = p[q];
+      v[2 * q] = x.x;
+      v[2 * q + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = 0.0;
+  }
+}
+
+// Persistent: one CTA per SM walks the work units (split-major, so that the
+// CTAs working at one time share row chunks in L2).  Per unit: raw FP64 rows
+// stream in by bulk copies two steps ahead of the digit stage; every thread
+// turns 16 values of one column into digits; one thread issues the 34 MMAs of
+// the step; TMEM accumulates the unit; the flush writes its FP64 partial.
+__global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  double *scaleA = reinterpret_cast<double *>(oz_smem + 2 * OZ_STAGE);
+  uint8_t *raw0 = oz_smem;                             // [2][OZ_RAW_STAGE]
+  uint8_t *dig0 = oz_smem + 2 * OZ_RAW_STAGE;          // [2][OZ_STAGE]
+  uint8_t *misc = dig0 + 2 * OZ_STAGE;
+  double *scaleA = reinterpret_cast<double *>(misc);
   double *scaleB = scaleA + 128;
   int *SA = reinterpret_cast<int *>(scaleB + 64);
   int *SB = SA + 128;
   int *badA = SB + 64;
   int *badB = badA + 128;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(badB + 64);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  uint64_t *full = reinterpret_cast<uint64_t *>(badB + 64);  // [2] raw stage loaded
+  uint64_t *mdone = full + 2;                                 // [2] MMAs of a digit stage done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // unit -> split, task, tile
-  const int split = blockIdx.x / g.ntiles;
-  int gt = blockIdx.x - split * g.ntiles;
-  int ti = 0;
-  while (ti + 1 < g.nt && g.t[ti + 1].tile0 <= gt) ++ti;
-  const OzTask &tk = g.t[ti];
-  int lt = gt - tk.tile0, ia = 0, jb = 0;
-  if (tk.sym) {  // tiles with 2 ia <= jb only (the rest comes from the transpose)
-    while (lt >= tk.tb - 2 * ia) {
-      lt -= tk.tb - 2 * ia;
-      ++ia;
-    }
-    jb = 2 * ia + lt;
-  } else {
-    ia = lt / tk.tb;
-    jb = lt - ia * tk.tb;
-  }
-  const long long r0 = (long long)split * chunk;
-  const long long r1 = min(tk.rows, r0 + chunk);
-  const int nsteps = r1 > r0 ? (int)((r1 - r0 + 31) / 32) : 0;
-
-  if (tid < 128) {
-    const int c = ia * 128 + tid;
-    double s = 1.0;
-    int S = 0;
-    bool fin = true;
-    if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin);
-    scaleA[tid] = s;
-    SA[tid] = S;
-    badA[tid] = !fin;
-  } else if (tid < 192) {
-    const int c = jb * 64 + tid - 128;
-    double s = 1.0;
-    int S = 0;
-    bool fin = true;
-    if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin);
-    scaleB[tid - 128] = s;
-    SB[tid - 128] = S;
-    badB[tid - 128] = !fin;
-  }
-  if (warp == 0 && nsteps > 0) tmem_alloc(tslot, 512);
+  if (warp == 0) tmem_alloc(tslot, 512);
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&mdone[i], 1);
+    }
     mbar_init_fence();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = nsteps > 0 ? *tslot : 0u;
+  const uint32_t tmem = *tslot;
+  uint32_t fph[2] = {0u, 0u}, mph[2] = {0u, 0u};
+  int failed = 0;
 
-  // this thread's columns: A column ca (all threads), B column cb (threads < 128)
-  const int ca = tid >> 1, ha = tid & 1;
-  const int cb = (tid & 127) >> 1, hb = tid & 1;
+  // digit roles: A column ca (rows 16 ha..), B column cb (threads < 128)
+  const int ca = tid & 127, ha = tid >> 7;
+  const int cb = tid & 63, hb = (tid >> 6) & 1;
   const bool hasB = tid < 128;
-  const bool va = ia * 128 + ca < tk.ka, vb = hasB && (jb * 64 + cb < tk.kb);
-  const double *colA = tk.a + (long long)(va ? ia * 128 + ca : 0) * tk.lda;
-  const double *colB = tk.b + (long long)(vb ? jb * 64 + cb : 0) * tk.ldb;
-  const double sa = scaleA[ca], sb = hasB ? scaleB[cb] : 1.0;
   const int offA = (ca & 7) * 16 + (ca >> 3) * 256 + ha * 128;
   const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + hb * 128;
 
-  double xa[16], xb[16];
-  if (nsteps > 0) {
-    oz_load16(colA, r0 + 16 * ha, r1, va, xa);
-    if (hasB) oz_load16(colB, r0 + 16 * hb, r1, vb, xb);
-  }
-  uint32_t ph[2] = {0u, 0u};
-  int failed = 0;
-  for (int ks = 0; ks < nsteps; ++ks) {
-    const int s = ks & 1;
-    // digits of this step from the registers, then the next step's loads
-    uint4 da[OZ_ND], db[OZ_ND];
-    oz_digits16(xa, sa, da);
-    if (hasB) oz_digits16(xb, sb, db);
-    if (ks + 1 < nsteps) {
-      const long long rn = r0 + (long long)(ks + 1) * 32;
-      oz_load16(colA, rn + 16 * ha, r1, va, xa);
-      if (hasB) oz_load16(colB, rn + 16 * hb, r1, vb, xb);
+  for (int unit = blockIdx.x; unit < nunits && !failed; unit += gridDim.x) {
+    const int split = unit / g.ntiles;
+    const int gt = unit - split * g.ntiles;
+    int ti = 0;
+    while (ti + 1 < g.nt && g.t[ti + 1].tile0 <= gt) ++ti;
+    const OzTask &tk = g.t[ti];
+    int lt = gt - tk.tile0, ia = 0, jb = 0;
+    if (tk.sym) {
+      while (lt >= tk.tb - 2 * ia) {
+        lt -= tk.tb - 2 * ia;
+        ++ia;
+      }
+      jb = 2 * ia + lt;
+    } else {
+      ia = lt / tk.tb;
+      jb = lt - ia * tk.tb;
     }
-    if (ks >= 2) {  // the MMAs committed two steps ago read this stage
-      const bool ok = mbar_wait(&bar[s], ph[s], TC_WAIT_LIMIT);
-      ph[s] ^= 1u;
+    const long long r0 = (long long)split * chunk;
+    const long long r1 = min(tk.rows, r0 + chunk);
+    const int nsteps = r1 > r0 ? (int)((r1 - r0) / 32) : 0;  // rows are a multiple of 32
+
+    if (tid < 128) {
+      const int c = ia * 128 + tid;
+      double s = 1.0;
+      int S = 0;
+      bool fin = true;
+      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin);
+      scaleA[tid] = s;
+      SA[tid] = S;
+      badA[tid] = !fin;
+    } else if (tid < 192) {
+      const int c = jb * 64 + tid - 128;
+      double s = 1.0;
+      int S = 0;
+      bool fin = true;
+      if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin);
+      scaleB[tid - 128] = s;
+      SB[tid - 128] = S;
+      badB[tid - 128] = !fin;
+    }
+    __syncthreads();
+    const bool va = ia * 128 + ca < tk.ka, vb = hasB && (jb * 64 + cb < tk.kb);
+    const double sa = scaleA[ca], sb = hasB ? scaleB[cb] : 1.0;
+    // prologue: raw stages for steps 0 and 1
+    if (warp == 0)
+      for (int k = 0; k < 2 && k < nsteps; ++k) oz_issue_step(tk, ia, jb, r0 + 32LL * k, raw0 + k * OZ_RAW_STAGE, &full[k], lane);
+
+    for (int ks = 0; ks < nsteps; ++ks) {
+      const int s = ks & 1;
+      uint8_t *raw = raw0 + s * OZ_RAW_STAGE;
+      uint8_t *dig = dig0 + s * OZ_STAGE;
+      bool ok = mbar_wait(&full[s], fph[s], TC_WAIT_LIMIT);
+      fph[s] ^= 1u;
+      if (ok && ks >= 2) {  // the MMAs of step ks - 2 read this digit stage
+        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
+        mph[s] ^= 1u;
+      }
+      failed = __syncthreads_or(!ok);
+      if (failed) break;
+      {
+        double v[16];
+        uint4 d[OZ_ND];
+        oz_raw16(raw, ca, ha, va, v);
+        oz_digits16(v, sa, d);
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + t * 4096 + offA) = d[t];
+        if (hasB) {
+          oz_raw16(raw + OZ_RAW_A, cb, hb, vb, v);
+          oz_digits16(v, sb, d);
+#pragma unroll
+          for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + OZ_STAGE_A + t * 2048 + offB) = d[t];
+        }
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (warp == 0) {
+        if (lane == 0) {
+          tc_fence_after();
+          const uint32_t id = idesc_i8(64);
+          const uint32_t base = smem_u32(dig);
+#pragma unroll
+          for (int t = 0; t < OZ_ND; ++t)
+#pragma unroll
+            for (int u = 0; u < OZ_ND; ++u) {
+              const int D = t + u;
+              if (D < OZ_DMIN) continue;
+              const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+              mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
+                     smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
+            }
+          mma_commit(&mdone[s]);
+        }
+        __syncwarp();
+        // the raw stage is consumed: refill it with step ks + 2
+        if (ks + 2 < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * (ks + 2), raw, &full[s], lane);
+      }
+    }
+    if (failed) break;
+    // wait for the last commit of each digit stage used by this unit
+    if (nsteps > 0) {
+      bool ok = true;
+      for (int k = nsteps >= 2 ? nsteps - 2 : 0; k < nsteps && ok; ++k) {
+        const int s = k & 1;
+        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
+        mph[s] ^= 1u;
+      }
       failed = __syncthreads_or(!ok);
       if (failed) break;
     }
-    uint8_t *st = oz_smem + s * OZ_STAGE;
-#pragma unroll
-    for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(st + t * 4096 + offA) = da[t];
-    if (hasB) {
-#pragma unroll
-      for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(st + OZ_STAGE_A + t * 2048 + offB) = db[t];
-    }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t id = idesc_i8(64);
-      const uint32_t base = smem_u32(st);
-#pragma unroll
-      for (int t = 0; t < OZ_ND; ++t)
-#pragma unroll
-        for (int u = 0; u < OZ_ND; ++u) {
-          const int D = t + u;
-          if (D < OZ_DMIN) continue;
-          const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-          mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
-                 smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
-        }
-      mma_commit(&bar[s]);
-    }
-  }
-  if (!failed && nsteps > 0) {  // the last commit covers all MMAs of the unit
-    const int s = (nsteps - 1) & 1;
-    const bool ok = mbar_wait(&bar[s], ph[s], TC_WAIT_LIMIT);
-    failed = __syncthreads_or(!ok);
-  }
-  tc_fence_after();
-  // flush: warp w reads TMEM lanes 32 (w % 4).., columns 32 (w / 4)..
-  const int row = 32 * (warp & 3) + lane;
-  const int i = ia * 128 + row;
-  const int kk = tk.ka * tk.kb;
-  double *part = g.part + tk.part0 + (long long)split * kk;
-  if (failed) {
-    if (tid == 0) atomicExch(g.err, 1);
-  } else {
+    tc_fence_after();
+    // flush: warp w reads TMEM lanes 32 (w % 4).., columns 32 (w / 4)..
+    const int row = 32 * (warp & 3) + lane;
+    const int i = ia * 128 + row;
+    const long long kk = (long long)tk.ka * tk.kb;
+    double *part = g.part + tk.part0 + (long long)split * kk;
     for (int grp = 0; grp < 2; ++grp) {
       const int c0 = 32 * (warp >> 2) + 16 * grp;
       double acc[16];
@@ -392,10 +461,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
         }
       }
     }
+    // TMEM reads and scale reads done before the next unit reuses them
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
+  if (failed && tid == 0) atomicExch(g.err, 1);
   tc_fence_before();
   __syncthreads();
-  if (warp == 0 && nsteps > 0) tmem_free(tmem, 512);
+  if (warp == 0) tmem_free(tmem, 512);
 }
 
 // |x| maxima of the columns of an operand (FP64 bit patterns, atomic max;
@@ -471,7 +545,7 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
   int tiles = 0;
   for (int i = 0; i < ntask; ++i) {
     const bdgd_gram_task &s = tasks[i];
-    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0)
+    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0 || s.rows % 32)
       return BDGD_ERR_UNSUPPORTED;
     OzTask &t = g.t[i];
     t.a = (const double *)s.a;
@@ -538,9 +612,15 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     BDGD_CK(cudaGetLastError());
   }
   if (!bdgd_capturing)
-    BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+    BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM2));
+  int nsm = 148;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  const int nunits = tiles * nsplit;
   bdgd_count_launch();
-  k_gram_oz<<<(unsigned)(tiles * nsplit), OZ_THREADS, OZ_SMEM, c->stream>>>(g, chunk);
+  k_gram_oz<<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_THREADS, OZ_SMEM2, c->stream>>>(g, chunk, nunits);
   BDGD_CK(cudaGetLastError());
   bdgd_count_launch();
   k_oz_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, ldo, d_out);
