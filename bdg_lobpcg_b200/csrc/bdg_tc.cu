@@ -227,37 +227,32 @@ __device__ __forceinline__ void oz_load16(const double *__restrict__ col, long l
   }
 }
 
-// bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
-// global to this CTA's shared memory, completing on the mbarrier's tx count
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
 // Raw FP64 stage: 32 rows of each of the tile's columns, column c at
-// c * OZ_RAW_LD bytes (272: 16-byte aligned for the bulk copies, and 68 words
+// c * OZ_RAW_LD bytes (272: 16-byte aligned for the 16-byte copies, and 68 words
 // apart so that 8 consecutive columns fall in 8 different bank groups).
 #define OZ_RAW_LD 272
 #define OZ_RAW_A (128 * OZ_RAW_LD)
 #define OZ_RAW_STAGE (OZ_RAW_A + 64 * OZ_RAW_LD)
 #define OZ_SMEM2 (2 * OZ_RAW_STAGE + 2 * OZ_STAGE + 4096)
 
-// issue the bulk copies of step `ks` of the unit into raw stage `st` (warp 0)
-__device__ __forceinline__ void oz_issue_step(const OzTask &tk, int ia, int jb, long long r, uint8_t *raw,
-                                              uint64_t *full, int lane) {
+// copies of step rows [r, r + 32) of the tile's columns into a raw stage, by
+// all threads in 16-byte pieces (16 per column), then one commit group
+__device__ __forceinline__ void oz_issue_step(const OzTask &tk, int ia, int jb, long long r, uint8_t *raw, int tid) {
   const int na = min(128, tk.ka - ia * 128), nb = min(64, tk.kb - jb * 64);
-  if (lane == 0) mbar_expect_tx(full, (uint32_t)(na + nb) * 256u);
-  __syncwarp();
-  for (int c = lane; c < na; c += 32)
-    bulk_g2s(raw + c * OZ_RAW_LD, tk.a + (long long)(ia * 128 + c) * tk.lda + r, 256u, full);
-  for (int c = lane; c < nb; c += 32)
-    bulk_g2s(raw + OZ_RAW_A + c * OZ_RAW_LD, tk.b + (long long)(jb * 64 + c) * tk.ldb + r, 256u, full);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    const int seg = tid + OZ_THREADS * k;
+    const int piece = seg & 15;
+    if (seg < 2048) {
+      const int c = seg >> 4;
+      if (c < na) cp_async16(raw + c * OZ_RAW_LD + piece * 16, tk.a + (long long)(ia * 128 + c) * tk.lda + r + 2 * piece);
+    } else {
+      const int c = (seg - 2048) >> 4;
+      if (c < nb)
+        cp_async16(raw + OZ_RAW_A + c * OZ_RAW_LD + piece * 16, tk.b + (long long)(jb * 64 + c) * tk.ldb + r + 2 * piece);
+    }
+  }
+  cp_async_commit();
 }
 
 // 16 doubles (rows 16 h .. 16 h + 15) of column c of a raw stage region
@@ -278,7 +273,7 @@ __device__ __forceinline__ void oz_raw16(const uint8_t *region, int c, int h, bo
 
 // Persistent: one CTA per SM walks the work units (split-major, so that the
 // CTAs working at one time share row chunks in L2).  Per unit: raw FP64 rows
-// stream in by bulk copies two steps ahead of the digit stage; every thread
+// stream in by cp.async, two steps ahead of the digit stage; every thread
 // turns 16 values of one column into digits; one thread issues the 34 MMAs of
 // the step; TMEM accumulates the unit; the flush writes its FP64 partial.
 __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
@@ -292,24 +287,20 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
   int *SB = SA + 128;
   int *badA = SB + 64;
   int *badB = badA + 128;
-  uint64_t *full = reinterpret_cast<uint64_t *>(badB + 64);  // [2] raw stage loaded
-  uint64_t *mdone = full + 2;                                 // [2] MMAs of a digit stage done
+  uint64_t *mdone = reinterpret_cast<uint64_t *>(badB + 64);  // [2] MMAs of a digit stage done
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) tmem_alloc(tslot, 512);
   if (tid == 0) {
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&mdone[i], 1);
-    }
+    for (int i = 0; i < 2; ++i) mbar_init(&mdone[i], 1);
     mbar_init_fence();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  uint32_t fph[2] = {0u, 0u}, mph[2] = {0u, 0u};
+  uint32_t mph[2] = {0u, 0u};
   int failed = 0;
 
   // digit roles: A column ca (rows 16 ha..), B column cb (threads < 128)
@@ -362,17 +353,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
     __syncthreads();
     const bool va = ia * 128 + ca < tk.ka, vb = hasB && (jb * 64 + cb < tk.kb);
     const double sa = scaleA[ca], sb = hasB ? scaleB[cb] : 1.0;
-    // prologue: raw stages for steps 0 and 1
-    if (warp == 0)
-      for (int k = 0; k < 2 && k < nsteps; ++k) oz_issue_step(tk, ia, jb, r0 + 32LL * k, raw0 + k * OZ_RAW_STAGE, &full[k], lane);
+    // prologue: raw stages for steps 0 and 1 (a commit group each, empty past the end)
+    for (int k = 0; k < 2; ++k) {
+      if (k < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * k, raw0 + k * OZ_RAW_STAGE, tid);
+      else cp_async_commit();
+    }
 
     for (int ks = 0; ks < nsteps; ++ks) {
       const int s = ks & 1;
       uint8_t *raw = raw0 + s * OZ_RAW_STAGE;
       uint8_t *dig = dig0 + s * OZ_STAGE;
-      bool ok = mbar_wait(&full[s], fph[s], TC_WAIT_LIMIT);
-      fph[s] ^= 1u;
-      if (ok && ks >= 2) {  // the MMAs of step ks - 2 read this digit stage
+      cp_async_wait<1>();  // this thread's copies of step ks are done (the newest group is step ks + 1)
+      bool ok = true;
+      if (ks >= 2) {  // the MMAs of step ks - 2 read this digit stage
         ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
         mph[s] ^= 1u;
       }
@@ -411,11 +404,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
             }
           mma_commit(&mdone[s]);
         }
-        __syncwarp();
-        // the raw stage is consumed: refill it with step ks + 2
-        if (ks + 2 < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * (ks + 2), raw, &full[s], lane);
       }
+      // the raw stage is consumed: refill it with step ks + 2
+      if (ks + 2 < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * (ks + 2), raw, tid);
+      else cp_async_commit();
     }
+    cp_async_wait<0>();
     if (failed) break;
     // wait for the last commit of each digit stage used by this unit
     if (nsteps > 0) {
@@ -641,208 +635,255 @@ extern "C" int bdgd_gram_oz_error(bdgd_ctx *c) {
 
 // ---------------------------------------------------------------------------
 // Basis update on the integer tensor cores: Y = alpha sum_b S_b C_b + beta Y
-// for real FP64 blocks (the interface of bdgd_block_update).  The same digit
-// scheme as the Gram with the roles turned: each ROW of S = [S_1 .. S_nt]
-// (over all its K = sum k_b columns) and each COLUMN of C are scaled by a
-// power of two from their maximum; 7 signed 8-bit digits each; diagonals
-// t + u >= 5 (34 MMAs per 32-wide K step) in 8 int32 TMEM accumulators.
-// A work unit is (output, 128-row tile, 64-column tile); C's digits for all K
-// steps stay in shared memory; S is read twice per unit (its row maxima,
-// then the digits), the second time from L2.
+// for real FP64 blocks (the interface of bdgd_block_update).
+//
+// With S = [S_1 .. S_nt] (n x K) and C stacked (K x ncol):  Y = (S D^-1)(D C)
+// with D = diag(2^S_j) from the column maxima of S (the Gram's pre-pass):
+// every column of S D^-1 is below 1/2 in magnitude and is written, like the
+// Gram's operands, as X = rint(. 2^55) in 7 signed 8-bit digits; each column
+// c of D C gets its own power of two f_c.  Then
+//   Y_rc = 2^(f_c - 110) sum_{t,u} 256^(t+u) sum_j d_t(X_rj) d_u(X'_jc),
+// exact int32 sums of int8 digit products on the tensor cores (diagonals
+// t + u >= 5, 34 MMAs per 32-wide K step, 8 TMEM accumulators); the error is
+// about K 2^-55 of the largest term, that of an FP64 dot product of length K.
+// Persistent CTAs: each owns one (output, 64-column tile), keeps the digits
+// of its D C block in shared memory and walks row tiles of 128 rows (the
+// CTAs that share a row tile run together, so S comes from L2 after the
+// first); S streams in by cp.async (32 columns x 128 rows per K step).
 // ---------------------------------------------------------------------------
-#define OZU_MAXK 256                   // K = sum k_b limit (8 steps of 32)
-#define OZU_SMEM_C (8 * OZ_ND * 64 * 32)  // C digits of up to 8 K steps
-#define OZU_SMEM_A (2 * OZ_ND * 128 * 32) // two stages of S digits
-#define OZU_SMEM (OZU_SMEM_C + OZU_SMEM_A + 4096)
+#define OZU_MAXK 192                       // K = sum k_b limit (6 steps of 32)
+#define OZU_RAW_LD 1040                    // bytes per raw column (128 rows + 16 bytes)
+#define OZU_RAW_STAGE (32 * OZU_RAW_LD)
+#define OZU_SMEM_C (6 * OZ_ND * 64 * 32)   // D C digits of up to 6 K steps
+#define OZU_SMEM_A (2 * OZ_ND * 128 * 32)  // two stages of S digits
+#define OZU_SMEM (OZU_SMEM_C + OZU_SMEM_A + 2 * OZU_RAW_STAGE + 4096)
 
 struct OzuTerm {
   const double *s, *c;
   int k, ldc, nst;  // columns, C leading dim, K steps of 32
+  int mx;           // offset of the column maxima of s
 };
 struct OzuOut {
   double *y;
   int ncol, nterm;
   double alpha, beta;
   OzuTerm t[3];
-  int nst;          // K steps over all terms
+  int nst, ktot;
 };
 struct OzuArgs {
   OzuOut o[4];
   int nout;
   int ct_out[64], ct_col[64], nct;  // (output, 64-column tile) pairs
   long long n, ld, nrt;
+  const unsigned long long *colmax;
   int *err;
 };
 
-// 16 values of row r: columns [j0, j0 + 16) of term tm (zero past k or n)
-__device__ __forceinline__ void ozu_load_row16(const OzuTerm &tm, long long ld, long long r, long long n, int j0,
-                                               double (&v)[16]) {
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int j = j0 + q;
-    v[q] = (r < n && j < tm.k) ? __ldg(tm.s + (long long)j * ld + r) : 0.0;
+// K step `st` of output o: its term b and first column j0 inside the term
+__device__ __forceinline__ void ozu_step_term(const OzuOut &o, int st, int &b, int &j0) {
+  b = 0;
+  while (b + 1 < o.nterm && st >= o.t[b].nst) {
+    st -= o.t[b].nst;
+    ++b;
   }
+  j0 = 32 * st;
+}
+
+// copies of K step st (32 columns x 128 rows of S) into a raw stage, by all
+// threads in 16-byte pieces (64 per column), then one commit group
+__device__ __forceinline__ void ozu_issue_step(const OzuOut &o, int st, long long r0, long long ld, uint8_t *raw,
+                                               int tid) {
+  int b, j0;
+  ozu_step_term(o, st, b, j0);
+  const OzuTerm &tm = o.t[b];
+  const int nj = min(32, tm.k - j0);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int seg = tid + OZ_THREADS * k;
+    const int j = seg >> 6, piece = seg & 63;
+    if (j < nj) cp_async16(raw + j * OZU_RAW_LD + piece * 16, tm.s + (long long)(j0 + j) * ld + r0 + 2 * piece);
+  }
+  cp_async_commit();
 }
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  uint8_t *cdig = oz_smem;                        // [step][digit][64 x 32]
-  uint8_t *adig = oz_smem + OZU_SMEM_C;           // [stage][digit][128 x 32]
-  double *rmax = reinterpret_cast<double *>(oz_smem + OZU_SMEM_C + OZU_SMEM_A);  // [2][128]
-  double *cmax = rmax + 256;                                                  // [2][64]
-  int *cexpo = reinterpret_cast<int *>(cmax + 128);                           // [64] column exponents
-  int *cbadf = cexpo + 64;                                                    // [64] non-finite columns
-  uint64_t *bar = reinterpret_cast<uint64_t *>(cbadf + 64);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  uint8_t *cdig = oz_smem;                                   // [step][digit][64 x 32]
+  uint8_t *adig = oz_smem + OZU_SMEM_C;                      // [stage][digit][128 x 32]
+  uint8_t *raw0 = adig + OZU_SMEM_A;                         // [stage][32 columns][128 rows]
+  double *sS = reinterpret_cast<double *>(raw0 + 2 * OZU_RAW_STAGE);  // [192] 2^(55 - S_j)
+  double *cm = sS + OZU_MAXK;                                // [2][64] column maxima of D C
+  int *fexp = reinterpret_cast<int *>(cm + 128);             // [64]
+  int *fbad = fexp + 64;                                     // [64]
+  uint64_t *mdone = reinterpret_cast<uint64_t *>(fbad + 64);  // [2] MMAs of a digit stage done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long unit = blockIdx.x;
-  const int ct = (int)(unit % u.nct);
-  const long long rt = unit / u.nct;
+  const int ct = blockIdx.x % u.nct;
+  const int rstep = gridDim.x / u.nct;  // CTAs per (output, column tile)
+  const int rfirst = blockIdx.x / u.nct;
   const OzuOut &o = u.o[u.ct_out[ct]];
   const int c0 = 64 * u.ct_col[ct];
-  const long long r0 = rt * 128;
   const long long n = u.n, ld = u.ld;
 
   if (warp == 0) tmem_alloc(tslot, 512);
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int i = 0; i < 2; ++i) mbar_init(&mdone[i], 1);
     mbar_init_fence();
   }
-  // C: column maxima over all K, then the digits of every K step
-  const int cc = tid & 63, ch = (tid >> 6) & 1;  // threads < 128
-  {
-    double m = 0.0;
-    if (tid < 128 && c0 + cc < o.ncol) {
-      for (int b = 0; b < o.nterm; ++b) {
-        const OzuTerm &tm = o.t[b];
-        const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
-        for (int j = ch; j < tm.k; j += 2) {
-          const double x = fabs(col[j]);
-          m = (x > m || x != x) ? x : m;
-        }
-      }
+  // column scales of S: 2^(55 - S_j) (oz_scale), per stacked column j; a
+  // non-finite column makes the whole output NaN through D C below
+  for (int j = tid; j < OZU_MAXK; j += blockDim.x) {
+    double sc = 1.0;
+    int E = 0;
+    bool fin = true;
+    int b = 0, jj = j;
+    while (b < o.nterm && jj >= o.t[b].k) {
+      jj -= o.t[b].k;
+      ++b;
     }
-    if (tid < 128) cmax[ch * 64 + cc] = m;
-  }
-  // S: row maxima over all K
-  const int rr = tid & 127, rh = tid >> 7;
-  {
-    double m = 0.0;
-    const long long r = r0 + rr;
-    if (r < n)
-      for (int b = 0; b < o.nterm; ++b) {
-        const OzuTerm &tm = o.t[b];
-        for (int j = rh; j < tm.k; j += 2) {
-          const double x = fabs(__ldg(tm.s + (long long)j * ld + r));
-          m = (x > m || x != x) ? x : m;
-        }
-      }
-    rmax[rh * 128 + rr] = m;
+    if (b < o.nterm) oz_scale(u.colmax[o.t[b].mx + jj], sc, E, fin);
+    sS[j] = fin ? sc : __longlong_as_double(0x7ff8000000000000LL);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  // scales
-  double cs = 1.0, rs = 1.0;
-  int cS = 0, rS = 0;
-  bool cbad = false, rbad = false;
-  {
-    const double m0 = cmax[cc], m1 = cmax[64 + cc];
-    const double mc = (m0 > m1 || m0 != m0) ? m0 : m1;
-    bool fin = true;
-    oz_scale((unsigned long long)__double_as_longlong(mc), cs, cS, fin);
-    cbad = !fin;
-    const double n0 = rmax[rr], n1 = rmax[128 + rr];
-    const double mr = (n0 > n1 || n0 != n0) ? n0 : n1;
-    oz_scale((unsigned long long)__double_as_longlong(mr), rs, rS, fin);
-    rbad = !fin;
-    if (tid < 64) {
-      cexpo[cc] = cS;
-      cbadf[cc] = cbad;
-    }
-  }
-  // C digits: thread (cc, ch) writes K rows [16 ch, 16 ch + 16) of every step
+  // D C for this CTA's 64 columns: (D C)_jc = C_jc 2^S_j = C_jc 2^55 / sS_j,
+  // exact; column maxima, then the digits of every K step
+  const int cc = tid & 63, ch = (tid >> 6) & 1;
   if (tid < 128) {
-    int step = 0;
+    double m = 0.0;
+    if (c0 + cc < o.ncol) {
+      int jg = 0;
+      for (int b = 0; b < o.nterm; ++b) {
+        const OzuTerm &tm = o.t[b];
+        const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
+        for (int j = ch; j < tm.k; j += 2) {
+          const double x = fabs(col[j] * 0x1p55 / sS[jg + j]);
+          m = (x > m || x != x) ? x : m;
+        }
+        jg += tm.k;
+      }
+    }
+    cm[ch * 64 + cc] = m;
+  }
+  __syncthreads();
+  if (tid < 128) {
+    const double a0 = cm[cc], a1 = cm[64 + cc];
+    const double mc = (a0 > a1 || a0 != a0) ? a0 : a1;
+    double fs = 1.0;
+    int F = 0;
+    bool fin = true;
+    oz_scale((unsigned long long)__double_as_longlong(mc), fs, F, fin);
+    if (tid < 64) {
+      fexp[cc] = F;
+      fbad[cc] = !fin;
+    }
+    int st = 0, jg = 0;
+    const bool vc = c0 + cc < o.ncol;
     for (int b = 0; b < o.nterm; ++b) {
       const OzuTerm &tm = o.t[b];
       const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
-      const bool vc = c0 + cc < o.ncol;
-      for (int s = 0; s < tm.nst; ++s, ++step) {
+      for (int s = 0; s < tm.nst; ++s, ++st) {
         double v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const int j = 32 * s + 16 * ch + q;
-          v[q] = (vc && j < tm.k) ? col[j] : 0.0;
+          v[q] = (vc && j < tm.k) ? col[j] * 0x1p55 / sS[jg + j] : 0.0;
         }
         uint4 d[OZ_ND];
-        oz_digits16(v, cs, d);
+        oz_digits16(v, fs, d);
         const int off = (cc & 7) * 16 + (cc >> 3) * 256 + ch * 128;
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t)
-          *reinterpret_cast<uint4 *>(cdig + (step * OZ_ND + t) * 2048 + off) = d[t];
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(cdig + (st * OZ_ND + t) * 2048 + off) = d[t];
       }
+      jg += tm.k;
     }
   }
-  // main loop over K steps: S digits (row rr, K columns [16 rh, 16 rh + 16))
+  __syncthreads();
+
+  // S digits role: row rr of the tile, K columns [16 rh, 16 rh + 16) of a step
+  const int rr = tid & 127, rh = tid >> 7;
   const int offA = (rr & 7) * 16 + (rr >> 3) * 256 + rh * 128;
-  uint32_t ph[2] = {0u, 0u};
+  uint32_t mph[2] = {0u, 0u};
   int failed = 0;
-  int step = 0;
-  for (int b = 0; b < o.nterm && !failed; ++b) {
-    const OzuTerm &tm = o.t[b];
-    for (int s = 0; s < tm.nst; ++s, ++step) {
-      const int st = step & 1;
-      double v[16];
-      ozu_load_row16(tm, ld, r0 + rr, n, 32 * s + 16 * rh, v);
-      uint4 d[OZ_ND];
-      oz_digits16(v, rs, d);
-      if (step >= 2) {
-        const bool ok = mbar_wait(&bar[st], ph[st], TC_WAIT_LIMIT);
-        ph[st] ^= 1u;
-        failed = __syncthreads_or(!ok);
-        if (failed) break;
+  const int nst = o.nst;
+  for (long long rt = rfirst; rt < u.nrt && !failed; rt += rstep) {
+    const long long r0 = rt * 128;
+    for (int k = 0; k < 2; ++k) {  // a commit group each, empty past the end
+      if (k < nst) ozu_issue_step(o, k, r0, ld, raw0 + k * OZU_RAW_STAGE, tid);
+      else cp_async_commit();
+    }
+    for (int st = 0; st < nst; ++st) {
+      const int s = st & 1;
+      uint8_t *raw = raw0 + s * OZU_RAW_STAGE;
+      uint8_t *dig = adig + s * (OZ_ND * 4096);
+      cp_async_wait<1>();  // this thread's copies of step st are done
+      bool ok = true;
+      if (st >= 2) {
+        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
+        mph[s] ^= 1u;
       }
-      uint8_t *sa = adig + st * (OZ_ND * 4096);
+      failed = __syncthreads_or(!ok);
+      if (failed) break;
+      {
+        int b, j0;
+        ozu_step_term(o, st, b, j0);
+        int jg = j0;
+        for (int q = 0; q < b; ++q) jg += o.t[q].k;
+        const int kb = o.t[b].k;
+        double v[16];
 #pragma unroll
-      for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(sa + t * 4096 + offA) = d[t];
+        for (int q = 0; q < 16; ++q) {
+          const int j = 16 * rh + q;
+          v[q] = (j0 + j < kb) ? *reinterpret_cast<const double *>(raw + j * OZU_RAW_LD + rr * 8) * sS[jg + j] : 0.0;
+        }
+        uint4 d[OZ_ND];
+        oz_digits16(v, 1.0, d);
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + t * 4096 + offA) = d[t];
+      }
       fence_async_smem();
       __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        const uint32_t id = idesc_i8(64);
-        const uint32_t abase = smem_u32(sa), bbase = smem_u32(cdig + step * OZ_ND * 2048);
+      if (warp == 0) {
+        if (lane == 0) {
+          tc_fence_after();
+          const uint32_t id = idesc_i8(64);
+          const uint32_t abase = smem_u32(dig), bbase = smem_u32(cdig + st * OZ_ND * 2048);
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t)
+          for (int t = 0; t < OZ_ND; ++t)
 #pragma unroll
-          for (int q = 0; q < OZ_ND; ++q) {
-            const int D = t + q;
-            if (D < OZ_DMIN) continue;
-            const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-            mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(abase + t * 4096), smem_desc(bbase + q * 2048),
-                   id, (step > 0 || t > first_t) ? 1u : 0u);
-          }
-        mma_commit(&bar[st]);
+            for (int q = 0; q < OZ_ND; ++q) {
+              const int D = t + q;
+              if (D < OZ_DMIN) continue;
+              const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+              mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(abase + t * 4096),
+                     smem_desc(bbase + q * 2048), id, (st > 0 || t > first_t) ? 1u : 0u);
+            }
+          mma_commit(&mdone[s]);
+        }
       }
+      // the raw stage is consumed: refill it with step st + 2
+      if (st + 2 < nst) ozu_issue_step(o, st + 2, r0, ld, raw, tid);
+      else cp_async_commit();
     }
-  }
-  const int nsteps = step;
-  if (!failed && nsteps > 0) {
-    const int st = (nsteps - 1) & 1;
-    const bool ok = mbar_wait(&bar[st], ph[st], TC_WAIT_LIMIT);
-    failed = __syncthreads_or(!ok);
-  }
-  tc_fence_after();
-  if (failed) {
-    if (tid == 0) atomicExch(u.err, 1);
-  } else if (nsteps > 0) {
+    cp_async_wait<0>();
+    if (failed) break;
+    {  // the last commit of each digit stage of this row tile
+      bool ok = true;
+      for (int k = nst >= 2 ? nst - 2 : 0; k < nst && ok; ++k) {
+        const int s = k & 1;
+        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
+        mph[s] ^= 1u;
+      }
+      failed = __syncthreads_or(!ok);
+      if (failed) break;
+    }
+    tc_fence_after();
     // flush: warp w has TMEM lanes (rows) 32 (w % 4).., output columns 32 (w / 4)..
     const int row = 32 * (warp & 3) + lane;
     const long long r = r0 + row;
-    // this thread's own row scale is row's: rr = tid & 127 = 32 (warp % 4) + lane
     for (int grp = 0; grp < 2; ++grp) {
       const int cl = 32 * (warp >> 2) + 16 * grp;
       double acc[16];
@@ -861,8 +902,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
         for (int q = 0; q < 16; ++q) {
           const int c = c0 + cl + q;
           if (c < o.ncol) {
-            double val = o.alpha * ldexp(acc[q], rS + cexpo[cl + q]);
-            if (rbad || cbadf[cl + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+            double val = o.alpha * ldexp(acc[q], fexp[cl + q]);
+            if (fbad[cl + q]) val = __longlong_as_double(0x7ff8000000000000LL);
             double *yp = o.y + (long long)c * ld + r;
             if (o.beta != 0.0) val += o.beta * *yp;
             *yp = val;
@@ -870,7 +911,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
         }
       }
     }
+    // TMEM reads done before the next row tile's MMAs overwrite it
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
+  if (failed && tid == 0) atomicExch(u.err, 1);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_free(tmem, 512);
@@ -880,12 +926,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
 // BDGD_ERR_UNSUPPORTED (nothing launched) outside its limits.
 extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int nout, const bdgd_update_out *outs) {
   if (nout <= 0 || n == 0) return BDGD_OK;
-  if (nout > 4 || ld < n) return BDGD_ERR_UNSUPPORTED;
+  if (nout > 4 || ld < n || n % 128 || ld % 2) return BDGD_ERR_UNSUPPORTED;
   OzuArgs u;
   memset(&u, 0, sizeof u);
   u.n = (long long)n;
   u.ld = (long long)ld;
   u.nout = nout;
+  struct Op {
+    const double *p;
+    int k, off;
+  } ops[12];
+  int nops = 0, moff = 0;
   for (int i = 0; i < nout; ++i) {
     const bdgd_update_out &s = outs[i];
     if (s.nterm < 0 || s.nterm > 3 || s.ncol < 0 || ((uintptr_t)s.y % 8)) return BDGD_ERR_UNSUPPORTED;
@@ -894,10 +945,9 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
     o.ncol = s.ncol;
     o.alpha = s.alpha;
     o.beta = s.beta;
-    int ktot = 0;
     for (int b = 0; b < s.nterm; ++b) {
       if (s.term[b].k <= 0) continue;
-      if (((uintptr_t)s.term[b].s % 8) || s.term[b].ldc < s.term[b].k || ((uintptr_t)s.term[b].c % 8))
+      if (((uintptr_t)s.term[b].s % 16) || s.term[b].ldc < s.term[b].k || ((uintptr_t)s.term[b].c % 8))
         return BDGD_ERR_UNSUPPORTED;
       OzuTerm &t = o.t[o.nterm++];
       t.s = (const double *)s.term[b].s;
@@ -906,9 +956,19 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
       t.ldc = s.term[b].ldc;
       t.nst = (t.k + 31) / 32;
       o.nst += t.nst;
-      ktot += t.k;
+      o.ktot += t.k;
+      int found = -1;
+      for (int q = 0; q < nops; ++q)
+        if (ops[q].p == t.s && ops[q].k == t.k) found = ops[q].off;
+      if (found < 0) {
+        ops[nops] = {t.s, t.k, moff};
+        found = moff;
+        moff += t.k;
+        nops++;
+      }
+      t.mx = found;
     }
-    if (o.nst > 8 || ktot > OZU_MAXK) return BDGD_ERR_UNSUPPORTED;
+    if (o.nst > 6 || o.ktot > OZU_MAXK) return BDGD_ERR_UNSUPPORTED;
     for (int j = 0; o.nterm > 0 && j * 64 < s.ncol; ++j) {  // no terms: Y untouched
       if (u.nct == 64) return BDGD_ERR_UNSUPPORTED;
       u.ct_out[u.nct] = i;
@@ -917,14 +977,35 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
     }
   }
   if (u.nct == 0) return BDGD_OK;
-  u.nrt = ((long long)n + 127) / 128;
-  int rc = bdgd_ensure(c->stream, &c->oz_buf, &c->oz_buf_bytes, 16);
+  u.nrt = (long long)n / 128;
+  const size_t mbytes = 16 + sizeof(unsigned long long) * (size_t)moff;
+  int rc = bdgd_ensure(c->stream, &c->oz_buf, &c->oz_buf_bytes, mbytes);
   if (rc) return rc;
   u.err = (int *)c->oz_buf;
+  unsigned long long *colmax = (unsigned long long *)((char *)c->oz_buf + 16);
+  u.colmax = colmax;
+  BDGD_CK(cudaMemsetAsync(c->oz_buf, 0, mbytes, c->stream));
+  for (int i = 0; i < nops; ++i) {
+    const long long span = 65536;
+    const unsigned ny = (unsigned)(((long long)n + span - 1) / span);
+    bdgd_count_launch();
+    k_oz_colmax<<<dim3((unsigned)ops[i].k, ny), 256, 0, c->stream>>>(ops[i].p, (long long)ld, (long long)n, span,
+                                                                    colmax + ops[i].off);
+    BDGD_CK(cudaGetLastError());
+  }
+  int nsm = 148;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  // persistent CTAs: the same count for every (output, column tile), at most one per SM
+  int per = nsm / u.nct;
+  if (per < 1) per = 1;
+  if ((long long)per > u.nrt) per = (int)u.nrt;
   if (!bdgd_capturing)
     BDGD_CK(cudaFuncSetAttribute(k_update_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZU_SMEM));
   bdgd_count_launch();
-  k_update_oz<<<(unsigned)(u.nrt * u.nct), OZ_THREADS, OZU_SMEM, c->stream>>>(u);
+  k_update_oz<<<(unsigned)(per * u.nct), OZ_THREADS, OZU_SMEM, c->stream>>>(u);
   BDGD_CK(cudaGetLastError());
   return BDGD_OK;
 }
