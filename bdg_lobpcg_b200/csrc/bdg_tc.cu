@@ -114,27 +114,24 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
 }
 
 // ---------------------------------------------------------------------------
-// FP64 Gram contraction on the integer tensor cores (Ozaki-style splitting).
+// FP64 contractions on the integer tensor cores (Ozaki-style splitting).
 //
-// C = A^T B over a long row range, A (rows x ka) and B (rows x kb) FP64,
-// column-major.  Each column c is scaled by a power of two 2^(55 - S_c) with
-// max_r |x_rc| < 2^(S_c - 1) (S_c from the column maximum, measured by a
-// pre-pass), rounded to a 54-bit integer X and written in 7 signed 8-bit
-// digits: X = sum_{t<6} d_t 256^t + d_6 256^6, taken from the bytes of
-// X + 0x808080808080 (the offset makes the six low digits signed).  Then
+// A value x of a column (or row) whose magnitudes stay below 2^(S-1) is
+// written as the integer X = rint(x 2^(55 - S)), |X| < 2^54, in 7 signed
+// 8-bit digits: X = sum_{t<6} d_t 256^t + d_6 256^6, taken from the bytes of
+// X + 0x808080808080 (the offset makes the six low digits signed).  A dot
+// product of two such sequences is
 //   sum_r a_r b_r = 2^(S_a + S_b - 110) sum_{t,u} 256^(t+u) sum_r d_t d'_u,
 // each inner sum an exact int32 dot product of int8 digits on the tensor
 // cores (tcgen05.mma kind::i8).  Diagonals t + u >= 5 are kept (34 MMAs per
-// 32-row step); the dropped ones are below 2^-57 of max|a| max|b| per row.
+// 32-deep step); the dropped ones are below 2^-57 of max|a| max|b| per term.
 // The 8 kept diagonals accumulate in 8 int32 TMEM accumulators (128 x 64
-// each, the whole 512 TMEM columns); a diagonal sums at most 7 products of
-// |d| <= 128 per row, so 16384 rows stay exact in int32.  Each work unit is
-// (task, 128 x 64 output tile, 16384-row chunk); its FP64 result goes to the
-// split partials that k_oz_reduce sums in a fixed order.
+// each: all 512 TMEM columns); a diagonal sums at most 7 products of
+// |d| <= 128 per term, so 16384 terms stay exact in int32.
 // ---------------------------------------------------------------------------
 #define OZ_CHUNK 16384
 #define OZ_MAXT 48
-#define OZ_THREADS 256
+#define OZ_THREADS 512
 #define OZ_ND 7          // digits per value
 #define OZ_DMIN 5        // lowest kept diagonal t + u
 #define OZ_NDIAG 8       // kept diagonals 5..12
@@ -142,26 +139,6 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
 #define OZ_STAGE_A (OZ_ND * 128 * 32)
 #define OZ_STAGE_B (OZ_ND * 64 * 32)
 #define OZ_STAGE (OZ_STAGE_A + OZ_STAGE_B)
-// dynamic shared memory: two stages plus bookkeeping, sized above half of an
-// SM's shared memory so that one CTA holds each SM (its TMEM is all taken)
-#define OZ_SMEM (120 * 1024)
-
-struct OzTask {
-  const double *a, *b;
-  long long lda, ldb, rows;
-  int ka, kb, out, i0, j0, sym, mirror;
-  int ta, tb, ntile, tile0;
-  int ma, mb;             // offsets of the operands' column maxima
-  long long part0;        // offset of the task's split partials (doubles)
-};
-
-struct OzArgs {
-  OzTask t[OZ_MAXT];
-  int nt, ntiles, nsplit;
-  const unsigned long long *colmax;  // |x| maxima as FP64 bit patterns
-  double *part;
-  int *err;
-};
 
 __device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale, int &S, bool &finite) {
   const double m = __longlong_as_double((long long)bits);
@@ -180,106 +157,123 @@ __device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale,
   scale = ldexp(1.0, p);
 }
 
-// digits of 16 consecutive values (rows) -> per digit t one 16-byte vector
-__device__ __forceinline__ void oz_digits16(const double (&v)[16], double scale, uint4 (&dig)[OZ_ND]) {
+// digit words of 4 consecutive values: w[t] holds digit t of the four
+__device__ __forceinline__ void oz_digits4(double v0, double v1, double v2, double v3, double scale,
+                                           uint32_t (&w)[OZ_ND]) {
+  uint32_t lo[4], hi[4];
+  const double v[4] = {v0, v1, v2, v3};
 #pragma unroll
-  for (int g = 0; g < 4; ++g) {
-    uint32_t lo[4], hi[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const long long X = __double2ll_rn(v[4 * g + q] * scale) + 0x808080808080LL;
-      lo[q] = (uint32_t)X ^ 0x80808080u;
-      hi[q] = (uint32_t)((unsigned long long)X >> 32) ^ 0x8080u;
-    }
-    // 4 x 4 byte transposes: word t holds digit t of the four values
-    const uint32_t a0 = __byte_perm(lo[0], lo[1], 0x5140), a1 = __byte_perm(lo[2], lo[3], 0x5140);
-    const uint32_t a2 = __byte_perm(lo[0], lo[1], 0x7362), a3 = __byte_perm(lo[2], lo[3], 0x7362);
-    const uint32_t b0 = __byte_perm(hi[0], hi[1], 0x5140), b1 = __byte_perm(hi[2], hi[3], 0x5140);
-    const uint32_t b2 = __byte_perm(hi[0], hi[1], 0x7362), b3 = __byte_perm(hi[2], hi[3], 0x7362);
-    const uint32_t w[OZ_ND] = {__byte_perm(a0, a1, 0x5410), __byte_perm(a0, a1, 0x7632), __byte_perm(a2, a3, 0x5410),
-                               __byte_perm(a2, a3, 0x7632), __byte_perm(b0, b1, 0x5410), __byte_perm(b0, b1, 0x7632),
-                               __byte_perm(b2, b3, 0x5410)};
-#pragma unroll
-    for (int t = 0; t < OZ_ND; ++t) {
-      if (g == 0) dig[t].x = w[t];
-      if (g == 1) dig[t].y = w[t];
-      if (g == 2) dig[t].z = w[t];
-      if (g == 3) dig[t].w = w[t];
-    }
+  for (int q = 0; q < 4; ++q) {
+    const long long X = __double2ll_rn(v[q] * scale) + 0x808080808080LL;
+    lo[q] = (uint32_t)X ^ 0x80808080u;
+    hi[q] = (uint32_t)((unsigned long long)X >> 32) ^ 0x8080u;
   }
+  // 4 x 4 byte transposes
+  const uint32_t a0 = __byte_perm(lo[0], lo[1], 0x5140), a1 = __byte_perm(lo[2], lo[3], 0x5140);
+  const uint32_t a2 = __byte_perm(lo[0], lo[1], 0x7362), a3 = __byte_perm(lo[2], lo[3], 0x7362);
+  const uint32_t b0 = __byte_perm(hi[0], hi[1], 0x5140), b1 = __byte_perm(hi[2], hi[3], 0x5140);
+  const uint32_t b2 = __byte_perm(hi[0], hi[1], 0x7362), b3 = __byte_perm(hi[2], hi[3], 0x7362);
+  w[0] = __byte_perm(a0, a1, 0x5410);
+  w[1] = __byte_perm(a0, a1, 0x7632);
+  w[2] = __byte_perm(a2, a3, 0x5410);
+  w[3] = __byte_perm(a2, a3, 0x7632);
+  w[4] = __byte_perm(b0, b1, 0x5410);
+  w[5] = __byte_perm(b0, b1, 0x7632);
+  w[6] = __byte_perm(b2, b3, 0x5410);
 }
 
-// 16 rows [r, r + 16) of one column, zero outside [.., rend) or for a column
-// outside the operand
-__device__ __forceinline__ void oz_load16(const double *__restrict__ col, long long r, long long rend, bool valid,
-                                          double (&v)[16]) {
-  if (valid && r + 16 <= rend) {
-    const double2 *p = reinterpret_cast<const double2 *>(col + r);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const double2 x = __ldg(p + q);
-      v[2 * q] = x.x;
-      v[2 * q + 1] = x.y;
-    }
-  } else {
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = (valid && r + q < rend) ? __ldg(col + r + q) : 0.0;
-  }
-}
+struct OzTask {
+  const double *a, *b;
+  long long lda, ldb, rows;
+  int ka, kb, out, i0, j0, sym, mirror;
+  int ta, tb, ntile, tile0;
+  int nsp;                // row chunks of this task
+  int ma, mb;             // offsets of the operands' column maxima
+  long long part0;        // offset of the task's chunk partials (doubles)
+};
+
+struct OzArgs {
+  OzTask t[OZ_MAXT];      // sorted by nsp, largest first
+  int nt, ntiles;
+  const unsigned long long *colmax;  // |x| maxima as FP64 bit patterns
+  double *part;
+  int *err;
+};
 
 // Raw FP64 stage: 32 rows of each of the tile's columns, column c at
-// c * OZ_RAW_LD bytes (272: 16-byte aligned for the 16-byte copies, and 68 words
-// apart so that 8 consecutive columns fall in 8 different bank groups).
+// c * OZ_RAW_LD bytes (272: 16-byte aligned for the 16-byte copies, and 68
+// words apart so that 8 consecutive columns fall in 8 different bank groups).
 #define OZ_RAW_LD 272
 #define OZ_RAW_A (128 * OZ_RAW_LD)
 #define OZ_RAW_STAGE (OZ_RAW_A + 64 * OZ_RAW_LD)
 #define OZ_SMEM2 (2 * OZ_RAW_STAGE + 2 * OZ_STAGE + 4096)
 
-// copies of step rows [r, r + 32) of the tile's columns into a raw stage, by
-// all threads in 16-byte pieces (16 per column), then one commit group
+// copies of rows [r, r + 32) of the tile's columns into a raw stage, by all
+// threads in 16-byte pieces (16 per column), then one commit group
 __device__ __forceinline__ void oz_issue_step(const OzTask &tk, int ia, int jb, long long r, uint8_t *raw, int tid) {
   const int na = min(128, tk.ka - ia * 128), nb = min(64, tk.kb - jb * 64);
 #pragma unroll
-  for (int k = 0; k < 12; ++k) {
+  for (int k = 0; k < 6; ++k) {
     const int seg = tid + OZ_THREADS * k;
     const int piece = seg & 15;
     if (seg < 2048) {
       const int c = seg >> 4;
-      if (c < na) cp_async16(raw + c * OZ_RAW_LD + piece * 16, tk.a + (long long)(ia * 128 + c) * tk.lda + r + 2 * piece);
+      if (c < na)
+        cp_async16(raw + c * OZ_RAW_LD + piece * 16, tk.a + (long long)(ia * 128 + c) * tk.lda + r + 2 * piece);
     } else {
       const int c = (seg - 2048) >> 4;
       if (c < nb)
-        cp_async16(raw + OZ_RAW_A + c * OZ_RAW_LD + piece * 16, tk.b + (long long)(jb * 64 + c) * tk.ldb + r + 2 * piece);
+        cp_async16(raw + OZ_RAW_A + c * OZ_RAW_LD + piece * 16,
+                   tk.b + (long long)(jb * 64 + c) * tk.ldb + r + 2 * piece);
     }
   }
   cp_async_commit();
 }
 
-// 16 doubles (rows 16 h .. 16 h + 15) of column c of a raw stage region
-__device__ __forceinline__ void oz_raw16(const uint8_t *region, int c, int h, bool valid, double (&v)[16]) {
-  if (valid) {
-    const double2 *p = reinterpret_cast<const double2 *>(region + c * OZ_RAW_LD + h * 128);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const double2 x = p[q];
-      v[2 * q] = x.x;
-      v[2 * q + 1] = x.y;
+// unit -> (task, tile, chunk): chunks ascending; in chunk range
+// [nsp_{i+1}, nsp_i) the tasks 0..i (sorted by nsp, largest first) are active
+__device__ __forceinline__ void oz_unit(const OzArgs &g, int unit, int &ti, int &ia, int &jb, int &split) {
+  int u = unit;
+  ti = 0;
+  ia = jb = split = 0;
+  for (int i = g.nt - 1; i >= 0; --i) {
+    const int lo = (i == g.nt - 1) ? 0 : g.t[i + 1].nsp, hi = g.t[i].nsp;
+    const int P = g.t[i].tile0 + g.t[i].ntile;  // tiles of tasks 0..i
+    const int cnt = (hi - lo) * P;
+    if (u < cnt) {
+      split = lo + u / P;
+      const int gt = u - (u / P) * P;
+      while (ti + 1 <= i && g.t[ti + 1].tile0 <= gt) ++ti;
+      const OzTask &tk = g.t[ti];
+      int lt = gt - tk.tile0;
+      if (tk.sym) {  // tiles with 2 ia <= jb only (the rest comes from the transpose)
+        while (lt >= tk.tb - 2 * ia) {
+          lt -= tk.tb - 2 * ia;
+          ++ia;
+        }
+        jb = 2 * ia + lt;
+      } else {
+        ia = lt / tk.tb;
+        jb = lt - ia * tk.tb;
+      }
+      return;
     }
-  } else {
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = 0.0;
+    u -= cnt;
   }
 }
 
-// Persistent: one CTA per SM walks the work units (split-major, so that the
-// CTAs working at one time share row chunks in L2).  Per unit: raw FP64 rows
-// stream in by cp.async, two steps ahead of the digit stage; every thread
-// turns 16 values of one column into digits; one thread issues the 34 MMAs of
-// the step; TMEM accumulates the unit; the flush writes its FP64 partial.
+// C = A^T B over a long row range, A (rows x ka) and B (rows x kb) FP64,
+// column-major, each column scaled by its maximum over all rows (pre-pass).
+// Persistent: one CTA per SM walks the work units (task, 128 x 64 output
+// tile, 16384-row chunk) chunk by chunk, so that the CTAs working at one
+// time share rows in L2.  Per unit: raw FP64 rows stream in by cp.async two
+// steps ahead; every thread turns 8 values of an A column and 4 of a B column
+// into digits; one thread issues the 34 MMAs of the step; TMEM accumulates
+// the unit; the flush writes its FP64 chunk partial.
 __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  uint8_t *raw0 = oz_smem;                             // [2][OZ_RAW_STAGE]
-  uint8_t *dig0 = oz_smem + 2 * OZ_RAW_STAGE;          // [2][OZ_STAGE]
+  uint8_t *raw0 = oz_smem;                     // [2][OZ_RAW_STAGE]
+  uint8_t *dig0 = oz_smem + 2 * OZ_RAW_STAGE;  // [2][OZ_STAGE]
   uint8_t *misc = dig0 + 2 * OZ_STAGE;
   double *scaleA = reinterpret_cast<double *>(misc);
   double *scaleB = scaleA + 128;
@@ -303,30 +297,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
   uint32_t mph[2] = {0u, 0u};
   int failed = 0;
 
-  // digit roles: A column ca (rows 16 ha..), B column cb (threads < 128)
-  const int ca = tid & 127, ha = tid >> 7;
-  const int cb = tid & 63, hb = (tid >> 6) & 1;
-  const bool hasB = tid < 128;
-  const int offA = (ca & 7) * 16 + (ca >> 3) * 256 + ha * 128;
-  const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + hb * 128;
+  // digit roles: A column ca rows [8 hq, 8 hq + 8); B column cb rows [4 he, 4 he + 4)
+  const int ca = tid & 127, hq = tid >> 7;
+  const int cb = tid & 63, he = tid >> 6;
+  const int offA = (ca & 7) * 16 + (ca >> 3) * 256 + (hq >> 1) * 128 + (hq & 1) * 8;
+  const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + (he >> 2) * 128 + (he & 3) * 4;
 
   for (int unit = blockIdx.x; unit < nunits && !failed; unit += gridDim.x) {
-    const int split = unit / g.ntiles;
-    const int gt = unit - split * g.ntiles;
-    int ti = 0;
-    while (ti + 1 < g.nt && g.t[ti + 1].tile0 <= gt) ++ti;
+    int ti, ia, jb, split;
+    oz_unit(g, unit, ti, ia, jb, split);
     const OzTask &tk = g.t[ti];
-    int lt = gt - tk.tile0, ia = 0, jb = 0;
-    if (tk.sym) {
-      while (lt >= tk.tb - 2 * ia) {
-        lt -= tk.tb - 2 * ia;
-        ++ia;
-      }
-      jb = 2 * ia + lt;
-    } else {
-      ia = lt / tk.tb;
-      jb = lt - ia * tk.tb;
-    }
     const long long r0 = (long long)split * chunk;
     const long long r1 = min(tk.rows, r0 + chunk);
     const int nsteps = r1 > r0 ? (int)((r1 - r0) / 32) : 0;  // rows are a multiple of 32
@@ -351,8 +331,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
       badB[tid - 128] = !fin;
     }
     __syncthreads();
-    const bool va = ia * 128 + ca < tk.ka, vb = hasB && (jb * 64 + cb < tk.kb);
-    const double sa = scaleA[ca], sb = hasB ? scaleB[cb] : 1.0;
+    const bool va = ia * 128 + ca < tk.ka, vb = jb * 64 + cb < tk.kb;
+    const double sa = scaleA[ca], sb = scaleB[cb];
     // prologue: raw stages for steps 0 and 1 (a commit group each, empty past the end)
     for (int k = 0; k < 2; ++k) {
       if (k < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * k, raw0 + k * OZ_RAW_STAGE, tid);
@@ -372,38 +352,46 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
       failed = __syncthreads_or(!ok);
       if (failed) break;
       {
-        double v[16];
-        uint4 d[OZ_ND];
-        oz_raw16(raw, ca, ha, va, v);
-        oz_digits16(v, sa, d);
+        uint32_t w0[OZ_ND], w1[OZ_ND];
+        if (va) {
+          const double2 *p = reinterpret_cast<const double2 *>(raw + ca * OZ_RAW_LD + hq * 64);
+          const double2 x0 = p[0], x1 = p[1], x2 = p[2], x3 = p[3];
+          oz_digits4(x0.x, x0.y, x1.x, x1.y, sa, w0);
+          oz_digits4(x2.x, x2.y, x3.x, x3.y, sa, w1);
+        } else {
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + t * 4096 + offA) = d[t];
-        if (hasB) {
-          oz_raw16(raw + OZ_RAW_A, cb, hb, vb, v);
-          oz_digits16(v, sb, d);
-#pragma unroll
-          for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + OZ_STAGE_A + t * 2048 + offB) = d[t];
+          for (int t = 0; t < OZ_ND; ++t) w0[t] = w1[t] = 0u;
         }
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint2 *>(dig + t * 4096 + offA) = make_uint2(w0[t], w1[t]);
+        if (vb) {
+          const double2 *p = reinterpret_cast<const double2 *>(raw + OZ_RAW_A + cb * OZ_RAW_LD + he * 32);
+          const double2 x0 = p[0], x1 = p[1];
+          oz_digits4(x0.x, x0.y, x1.x, x1.y, sb, w0);
+        } else {
+#pragma unroll
+          for (int t = 0; t < OZ_ND; ++t) w0[t] = 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint32_t *>(dig + OZ_STAGE_A + t * 2048 + offB) = w0[t];
       }
       fence_async_smem();
       __syncthreads();
-      if (warp == 0) {
-        if (lane == 0) {
-          tc_fence_after();
-          const uint32_t id = idesc_i8(64);
-          const uint32_t base = smem_u32(dig);
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t id = idesc_i8(64);
+        const uint32_t base = smem_u32(dig);
 #pragma unroll
-          for (int t = 0; t < OZ_ND; ++t)
+        for (int t = 0; t < OZ_ND; ++t)
 #pragma unroll
-            for (int u = 0; u < OZ_ND; ++u) {
-              const int D = t + u;
-              if (D < OZ_DMIN) continue;
-              const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-              mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
-                     smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
-            }
-          mma_commit(&mdone[s]);
-        }
+          for (int u = 0; u < OZ_ND; ++u) {
+            const int D = t + u;
+            if (D < OZ_DMIN) continue;
+            const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+            mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
+                   smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
+          }
+        mma_commit(&mdone[s]);
       }
       // the raw stage is consumed: refill it with step ks + 2
       if (ks + 2 < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * (ks + 2), raw, tid);
@@ -423,39 +411,37 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
       if (failed) break;
     }
     tc_fence_after();
-    // flush: warp w reads TMEM lanes 32 (w % 4).., columns 32 (w / 4)..
+    // flush: warp w reads TMEM lanes 32 (w % 4).., columns 16 (w / 4)..
     const int row = 32 * (warp & 3) + lane;
     const int i = ia * 128 + row;
     const long long kk = (long long)tk.ka * tk.kb;
     double *part = g.part + tk.part0 + (long long)split * kk;
-    for (int grp = 0; grp < 2; ++grp) {
-      const int c0 = 32 * (warp >> 2) + 16 * grp;
-      double acc[16];
+    const int c0 = 16 * (warp >> 2);
+    double acc[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-      if (nsteps > 0) {
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    if (nsteps > 0) {
 #pragma unroll
-        for (int d = 0; d < OZ_NDIAG; ++d) {
-          int32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
-          const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+      for (int d = 0; d < OZ_NDIAG; ++d) {
+        int32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
+        const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
 #pragma unroll
-          for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
-        }
+        for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
       }
-      if (i < tk.ka) {
+    }
+    if (i < tk.ka) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int j = jb * 64 + c0 + q;
-          if (j < tk.kb) {
-            double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
-            if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
-            part[(long long)j * tk.ka + i] = val;
-          }
+      for (int q = 0; q < 16; ++q) {
+        const int j = jb * 64 + c0 + q;
+        if (j < tk.kb) {
+          double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
+          if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+          part[(long long)j * tk.ka + i] = val;
         }
       }
     }
-    // TMEM reads and scale reads done before the next unit reuses them
+    // TMEM and scale reads done before the next unit reuses them
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -491,7 +477,7 @@ __global__ void k_oz_colmax(const double *__restrict__ a, long long lda, long lo
   }
 }
 
-// sum of the split partials in fixed order; symmetric tasks take the
+// sum of the chunk partials in fixed order; symmetric tasks take the
 // transposed element where its tile was not computed; mirror writes C^T too
 __global__ void k_oz_reduce(OzArgs g, int ldo, double *__restrict__ outbuf) {
   const OzTask &tk = g.t[blockIdx.y];
@@ -505,11 +491,20 @@ __global__ void k_oz_reduce(OzArgs g, int ldo, double *__restrict__ outbuf) {
     }
     const double *pp = g.part + tk.part0 + (long long)sj * tk.ka + si;
     double s = 0.0;
-    for (int sp = 0; sp < g.nsplit; ++sp) s += pp[(long long)sp * kk];
+    for (int sp = 0; sp < tk.nsp; ++sp) s += pp[(long long)sp * kk];
     double *o = outbuf + (long long)tk.out * ldo * ldo;
     o[(long long)(tk.j0 + j) * ldo + tk.i0 + i] = s;
     if (tk.mirror) o[(long long)(tk.i0 + i) * ldo + tk.j0 + j] = s;
   }
+}
+
+static int oz_sm_count(bdgd_ctx *c) {
+  int nsm = 148;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  return nsm;
 }
 
 // Real FP64 task list on the tensor cores; BDGD_ERR_UNSUPPORTED (nothing
@@ -517,9 +512,25 @@ __global__ void k_oz_reduce(OzArgs g, int ldo, double *__restrict__ outbuf) {
 extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out) {
   if (ntask <= 0) return BDGD_OK;
   if (ntask > OZ_MAXT) return BDGD_ERR_UNSUPPORTED;
+  long long maxrows = 0;
+  for (int i = 0; i < ntask; ++i) {
+    const bdgd_gram_task &s = tasks[i];
+    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0 || s.rows % 32)
+      return BDGD_ERR_UNSUPPORTED;
+    if ((long long)s.rows > maxrows) maxrows = (long long)s.rows;
+  }
   OzArgs g;
   memset(&g, 0, sizeof g);
   g.nt = ntask;
+  // tasks in order of decreasing rows (so that chunk counts decrease)
+  int order[OZ_MAXT];
+  for (int i = 0; i < ntask; ++i) order[i] = i;
+  for (int i = 1; i < ntask; ++i)
+    for (int j = i; j > 0 && tasks[order[j]].rows > tasks[order[j - 1]].rows; --j) {
+      const int t = order[j];
+      order[j] = order[j - 1];
+      order[j - 1] = t;
+    }
   // unique operands (pointer, leading dimension, rows, columns) -> column maxima
   struct Op {
     const double *p;
@@ -535,13 +546,10 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     moff += k;
     return ops[nops++].off;
   };
-  long long maxrows = 0;
   int tiles = 0;
-  for (int i = 0; i < ntask; ++i) {
-    const bdgd_gram_task &s = tasks[i];
-    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0 || s.rows % 32)
-      return BDGD_ERR_UNSUPPORTED;
-    OzTask &t = g.t[i];
+  for (int q = 0; q < ntask; ++q) {
+    const bdgd_gram_task &s = tasks[order[q]];
+    OzTask &t = g.t[q];
     t.a = (const double *)s.a;
     t.b = (const double *)s.b;
     t.lda = (long long)s.lda;
@@ -566,25 +574,26 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     tiles += t.ntile;
     t.ma = op_index(s.a, s.lda, s.rows, s.ka);
     t.mb = op_index(s.b, s.ldb, s.rows, s.kb);
-    if (t.rows > maxrows) maxrows = t.rows;
   }
   g.ntiles = tiles;
   // row chunks: at most OZ_CHUNK rows (int32 exactness), enough units to fill the GPU
-  int nsplit = (2 * 148 + tiles - 1) / tiles;
+  const int nsm = oz_sm_count(c);
+  long long nsplit = (2LL * nsm + tiles - 1) / tiles;
   const long long minsplit = (maxrows + OZ_CHUNK - 1) / OZ_CHUNK;
   const long long maxsplit = (maxrows + 255) / 256;
-  if (nsplit < minsplit) nsplit = (int)minsplit;
-  if (nsplit > maxsplit) nsplit = (int)(maxsplit > minsplit ? maxsplit : minsplit);
+  if (nsplit < minsplit) nsplit = minsplit;
+  if (nsplit > maxsplit) nsplit = maxsplit > minsplit ? maxsplit : minsplit;
   if (nsplit < 1) nsplit = 1;
   long long chunk = (maxrows + nsplit - 1) / nsplit;
   chunk = (chunk + 31) / 32 * 32;
-  nsplit = (int)((maxrows + chunk - 1) / chunk);
-  if (nsplit < 1) nsplit = 1;
-  g.nsplit = nsplit;
   long long off = 0;
-  for (int i = 0; i < ntask; ++i) {
-    g.t[i].part0 = off;
-    off += (long long)nsplit * g.t[i].ka * g.t[i].kb;
+  int nunits = 0;
+  for (int q = 0; q < ntask; ++q) {
+    OzTask &t = g.t[q];
+    t.nsp = (int)((t.rows + chunk - 1) / chunk);
+    t.part0 = off;
+    off += (long long)t.nsp * t.ka * t.kb;
+    nunits += t.nsp * t.ntile;
   }
   int rc = bdgd_ensure(c->stream, (void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
   if (rc) return rc;
@@ -607,12 +616,6 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
   }
   if (!bdgd_capturing)
     BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM2));
-  int nsm = 148;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) {
-    cudaGetLastError();
-    nsm = 148;
-  }
-  const int nunits = tiles * nsplit;
   bdgd_count_launch();
   k_gram_oz<<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_THREADS, OZ_SMEM2, c->stream>>>(g, chunk, nunits);
   BDGD_CK(cudaGetLastError());
@@ -622,8 +625,8 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
   return BDGD_OK;
 }
 
-// the error flag of the last tensor-core Gram on this context (1: a wait on
-// the tensor core timed out); reads it synchronously
+// the error flag of the last tensor-core Gram or update on this context (1:
+// a wait on the tensor core timed out); reads it synchronously
 extern "C" int bdgd_gram_oz_error(bdgd_ctx *c) {
   if (!c->oz_buf || c->oz_buf_bytes < 16) return 0;
   int h = 0;
@@ -638,25 +641,23 @@ extern "C" int bdgd_gram_oz_error(bdgd_ctx *c) {
 // for real FP64 blocks (the interface of bdgd_block_update).
 //
 // With S = [S_1 .. S_nt] (n x K) and C stacked (K x ncol):  Y = (S D^-1)(D C)
-// with D = diag(2^S_j) from the column maxima of S (the Gram's pre-pass):
-// every column of S D^-1 is below 1/2 in magnitude and is written, like the
-// Gram's operands, as X = rint(. 2^55) in 7 signed 8-bit digits; each column
-// c of D C gets its own power of two f_c.  Then
-//   Y_rc = 2^(f_c - 110) sum_{t,u} 256^(t+u) sum_j d_t(X_rj) d_u(X'_jc),
-// exact int32 sums of int8 digit products on the tensor cores (diagonals
-// t + u >= 5, 34 MMAs per 32-wide K step, 8 TMEM accumulators); the error is
-// about K 2^-55 of the largest term, that of an FP64 dot product of length K.
-// Persistent CTAs: each owns one (output, 64-column tile), keeps the digits
-// of its D C block in shared memory and walks row tiles of 128 rows (the
-// CTAs that share a row tile run together, so S comes from L2 after the
-// first); S streams in by cp.async (32 columns x 128 rows per K step).
+// with D = diag(2^S_j) from the column maxima of S: every column of S D^-1
+// is written in the digits above with its own power of two, and each column
+// c of D C gets its own power of two f_c, so that
+//   Y_rc = 2^(f_c - 110) sum_{t,u} 256^(t+u) sum_j d_t(X_rj) d_u(X'_jc);
+// the error is about K 2^-55 of the largest term, that of an FP64 dot
+// product of length K.  Persistent CTAs: each owns one (output, 64-column
+// tile), keeps the digits of its D C block in shared memory and walks row
+// tiles of 128 rows (the CTAs that share a row tile run together, so S comes
+// from L2 after the first); S streams in by cp.async (32 columns x 128 rows
+// per K step), the next row tile's first steps during the current flush.
 // ---------------------------------------------------------------------------
 #define OZU_MAXK 192                       // K = sum k_b limit (6 steps of 32)
 #define OZU_RAW_LD 1040                    // bytes per raw column (128 rows + 16 bytes)
 #define OZU_RAW_STAGE (32 * OZU_RAW_LD)
 #define OZU_SMEM_C (6 * OZ_ND * 64 * 32)   // D C digits of up to 6 K steps
 #define OZU_SMEM_A (2 * OZ_ND * 128 * 32)  // two stages of S digits
-#define OZU_SMEM (OZU_SMEM_C + OZU_SMEM_A + 2 * OZU_RAW_STAGE + 4096)
+#define OZU_SMEM (OZU_SMEM_C + OZU_SMEM_A + 2 * OZU_RAW_STAGE + 8192)
 
 struct OzuTerm {
   const double *s, *c;
@@ -698,7 +699,7 @@ __device__ __forceinline__ void ozu_issue_step(const OzuOut &o, int st, long lon
   const OzuTerm &tm = o.t[b];
   const int nj = min(32, tm.k - j0);
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
+  for (int k = 0; k < 4; ++k) {
     const int seg = tid + OZ_THREADS * k;
     const int j = seg >> 6, piece = seg & 63;
     if (j < nj) cp_async16(raw + j * OZU_RAW_LD + piece * 16, tm.s + (long long)(j0 + j) * ld + r0 + 2 * piece);
@@ -712,10 +713,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
   uint8_t *adig = oz_smem + OZU_SMEM_C;                      // [stage][digit][128 x 32]
   uint8_t *raw0 = adig + OZU_SMEM_A;                         // [stage][32 columns][128 rows]
   double *sS = reinterpret_cast<double *>(raw0 + 2 * OZU_RAW_STAGE);  // [192] 2^(55 - S_j)
-  double *cm = sS + OZU_MAXK;                                // [2][64] column maxima of D C
-  int *fexp = reinterpret_cast<int *>(cm + 128);             // [64]
+  double *cm = sS + OZU_MAXK;                                // [8][64] partial column maxima of D C
+  int *fexp = reinterpret_cast<int *>(cm + 512);             // [64]
   int *fbad = fexp + 64;                                     // [64]
-  uint64_t *mdone = reinterpret_cast<uint64_t *>(fbad + 64);  // [2] MMAs of a digit stage done
+  double *fsc = reinterpret_cast<double *>(fbad + 64);       // [64] 2^(55 - f_c)
+  uint64_t *mdone = reinterpret_cast<uint64_t *>(fsc + 64);  // [2] MMAs of a digit stage done
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -725,14 +727,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
   const OzuOut &o = u.o[u.ct_out[ct]];
   const int c0 = 64 * u.ct_col[ct];
   const long long n = u.n, ld = u.ld;
+  const int nst = o.nst;
 
   if (warp == 0) tmem_alloc(tslot, 512);
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) mbar_init(&mdone[i], 1);
     mbar_init_fence();
   }
-  // column scales of S: 2^(55 - S_j) (oz_scale), per stacked column j; a
-  // non-finite column makes the whole output NaN through D C below
+  // the first row tile's first two K steps start loading now
+  long long G = 0;  // K steps issued so far, over this CTA's row tiles
+  auto issue_global = [&](long long Gs) {
+    const long long rt = rfirst + (Gs / nst) * rstep;
+    if (rt < u.nrt) ozu_issue_step(o, (int)(Gs % nst), rt * 128, ld, raw0 + (Gs & 1) * OZU_RAW_STAGE, tid);
+    else cp_async_commit();
+  };
+  issue_global(0);
+  issue_global(1);
+  // column scales of S: 2^(55 - S_j) per stacked column j; a non-finite
+  // column makes the whole output NaN through D C below
   for (int j = tid; j < OZU_MAXK; j += blockDim.x) {
     double sc = 1.0;
     int E = 0;
@@ -751,75 +763,76 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
   const uint32_t tmem = *tslot;
   // D C for this CTA's 64 columns: (D C)_jc = C_jc 2^S_j = C_jc 2^55 / sS_j,
   // exact; column maxima, then the digits of every K step
-  const int cc = tid & 63, ch = (tid >> 6) & 1;
-  if (tid < 128) {
+  const int cc = tid & 63, cp = tid >> 6;  // column, part 0..7
+  const bool vc = c0 + cc < o.ncol;
+  {
     double m = 0.0;
-    if (c0 + cc < o.ncol) {
+    if (vc) {
       int jg = 0;
       for (int b = 0; b < o.nterm; ++b) {
         const OzuTerm &tm = o.t[b];
         const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
-        for (int j = ch; j < tm.k; j += 2) {
+        for (int j = cp; j < tm.k; j += 8) {
           const double x = fabs(col[j] * 0x1p55 / sS[jg + j]);
           m = (x > m || x != x) ? x : m;
         }
         jg += tm.k;
       }
     }
-    cm[ch * 64 + cc] = m;
+    cm[cp * 64 + cc] = m;
   }
   __syncthreads();
-  if (tid < 128) {
-    const double a0 = cm[cc], a1 = cm[64 + cc];
-    const double mc = (a0 > a1 || a0 != a0) ? a0 : a1;
+  if (tid < 64) {
+    double mc = 0.0;
+    for (int q = 0; q < 8; ++q) {
+      const double a = cm[q * 64 + tid];
+      mc = (a > mc || a != a) ? a : mc;
+    }
     double fs = 1.0;
     int F = 0;
     bool fin = true;
     oz_scale((unsigned long long)__double_as_longlong(mc), fs, F, fin);
-    if (tid < 64) {
-      fexp[cc] = F;
-      fbad[cc] = !fin;
-    }
+    fexp[tid] = F;
+    fbad[tid] = !fin;
+    fsc[tid] = fs;
+  }
+  __syncthreads();
+  {  // thread (cc, cp): K rows [4 cp, 4 cp + 4) of every step
+    const double fs = fsc[cc];
+    const int off = (cc & 7) * 16 + (cc >> 3) * 256 + (cp >> 2) * 128 + (cp & 3) * 4;
     int st = 0, jg = 0;
-    const bool vc = c0 + cc < o.ncol;
     for (int b = 0; b < o.nterm; ++b) {
       const OzuTerm &tm = o.t[b];
       const double *col = tm.c + (long long)(c0 + cc) * tm.ldc;
       for (int s = 0; s < tm.nst; ++s, ++st) {
-        double v[16];
+        double v[4];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int j = 32 * s + 16 * ch + q;
+        for (int q = 0; q < 4; ++q) {
+          const int j = 32 * s + 4 * cp + q;
           v[q] = (vc && j < tm.k) ? col[j] * 0x1p55 / sS[jg + j] : 0.0;
         }
-        uint4 d[OZ_ND];
-        oz_digits16(v, fs, d);
-        const int off = (cc & 7) * 16 + (cc >> 3) * 256 + ch * 128;
+        uint32_t w[OZ_ND];
+        oz_digits4(v[0], v[1], v[2], v[3], fs, w);
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(cdig + (st * OZ_ND + t) * 2048 + off) = d[t];
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint32_t *>(cdig + (st * OZ_ND + t) * 2048 + off) = w[t];
       }
       jg += tm.k;
     }
   }
   __syncthreads();
 
-  // S digits role: row rr of the tile, K columns [16 rh, 16 rh + 16) of a step
-  const int rr = tid & 127, rh = tid >> 7;
-  const int offA = (rr & 7) * 16 + (rr >> 3) * 256 + rh * 128;
+  // S digits role: row rr of the tile, K columns [8 q4, 8 q4 + 8) of a step
+  const int rr = tid & 127, q4 = tid >> 7;
+  const int offA = (rr & 7) * 16 + (rr >> 3) * 256 + (q4 >> 1) * 128 + (q4 & 1) * 8;
   uint32_t mph[2] = {0u, 0u};
   int failed = 0;
-  const int nst = o.nst;
   for (long long rt = rfirst; rt < u.nrt && !failed; rt += rstep) {
     const long long r0 = rt * 128;
-    for (int k = 0; k < 2; ++k) {  // a commit group each, empty past the end
-      if (k < nst) ozu_issue_step(o, k, r0, ld, raw0 + k * OZU_RAW_STAGE, tid);
-      else cp_async_commit();
-    }
-    for (int st = 0; st < nst; ++st) {
+    for (int st = 0; st < nst; ++st, ++G) {
       const int s = st & 1;
-      uint8_t *raw = raw0 + s * OZU_RAW_STAGE;
+      const uint8_t *raw = raw0 + (G & 1) * OZU_RAW_STAGE;
       uint8_t *dig = adig + s * (OZ_ND * 4096);
-      cp_async_wait<1>();  // this thread's copies of step st are done
+      cp_async_wait<1>();  // this thread's copies of step G are done (the newest group is G + 1)
       bool ok = true;
       if (st >= 2) {
         ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
@@ -833,42 +846,40 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
         int jg = j0;
         for (int q = 0; q < b; ++q) jg += o.t[q].k;
         const int kb = o.t[b].k;
-        double v[16];
+        double v[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int j = 16 * rh + q;
+        for (int q = 0; q < 8; ++q) {
+          const int j = 8 * q4 + q;
           v[q] = (j0 + j < kb) ? *reinterpret_cast<const double *>(raw + j * OZU_RAW_LD + rr * 8) * sS[jg + j] : 0.0;
         }
-        uint4 d[OZ_ND];
-        oz_digits16(v, 1.0, d);
+        uint32_t w0[OZ_ND], w1[OZ_ND];
+        oz_digits4(v[0], v[1], v[2], v[3], 1.0, w0);
+        oz_digits4(v[4], v[5], v[6], v[7], 1.0, w1);
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint4 *>(dig + t * 4096 + offA) = d[t];
+        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint2 *>(dig + t * 4096 + offA) = make_uint2(w0[t], w1[t]);
       }
       fence_async_smem();
       __syncthreads();
-      if (warp == 0) {
-        if (lane == 0) {
-          tc_fence_after();
-          const uint32_t id = idesc_i8(64);
-          const uint32_t abase = smem_u32(dig), bbase = smem_u32(cdig + st * OZ_ND * 2048);
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t id = idesc_i8(64);
+        const uint32_t abase = smem_u32(dig), bbase = smem_u32(cdig + st * OZ_ND * 2048);
 #pragma unroll
-          for (int t = 0; t < OZ_ND; ++t)
+        for (int t = 0; t < OZ_ND; ++t)
 #pragma unroll
-            for (int q = 0; q < OZ_ND; ++q) {
-              const int D = t + q;
-              if (D < OZ_DMIN) continue;
-              const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-              mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(abase + t * 4096),
-                     smem_desc(bbase + q * 2048), id, (st > 0 || t > first_t) ? 1u : 0u);
-            }
-          mma_commit(&mdone[s]);
-        }
+          for (int q = 0; q < OZ_ND; ++q) {
+            const int D = t + q;
+            if (D < OZ_DMIN) continue;
+            const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+            mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(abase + t * 4096),
+                   smem_desc(bbase + q * 2048), id, (st > 0 || t > first_t) ? 1u : 0u);
+          }
+        mma_commit(&mdone[s]);
       }
-      // the raw stage is consumed: refill it with step st + 2
-      if (st + 2 < nst) ozu_issue_step(o, st + 2, r0, ld, raw, tid);
-      else cp_async_commit();
+      // the raw stage of step G is consumed: refill it with step G + 2 (maybe
+      // of the next row tile, loading while this tile is flushed)
+      issue_global(G + 2);
     }
-    cp_async_wait<0>();
     if (failed) break;
     {  // the last commit of each digit stage of this row tile
       bool ok = true;
@@ -881,33 +892,31 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
       if (failed) break;
     }
     tc_fence_after();
-    // flush: warp w has TMEM lanes (rows) 32 (w % 4).., output columns 32 (w / 4)..
+    // flush: warp w has TMEM lanes (rows) 32 (w % 4).., output columns 16 (w / 4)..
     const int row = 32 * (warp & 3) + lane;
     const long long r = r0 + row;
-    for (int grp = 0; grp < 2; ++grp) {
-      const int cl = 32 * (warp >> 2) + 16 * grp;
-      double acc[16];
+    const int cl = 16 * (warp >> 2);
+    double acc[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
 #pragma unroll
-      for (int d = 0; d < OZ_NDIAG; ++d) {
-        int32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + cl), v);
-        const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+    for (int d = 0; d < OZ_NDIAG; ++d) {
+      int32_t v[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + cl), v);
+      const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
-      }
-      if (r < n) {
+      for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
+    }
+    if (r < n) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int c = c0 + cl + q;
-          if (c < o.ncol) {
-            double val = o.alpha * ldexp(acc[q], fexp[cl + q]);
-            if (fbad[cl + q]) val = __longlong_as_double(0x7ff8000000000000LL);
-            double *yp = o.y + (long long)c * ld + r;
-            if (o.beta != 0.0) val += o.beta * *yp;
-            *yp = val;
-          }
+      for (int q = 0; q < 16; ++q) {
+        const int c = c0 + cl + q;
+        if (c < o.ncol) {
+          double val = o.alpha * ldexp(acc[q], fexp[cl + q]);
+          if (fbad[cl + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+          double *yp = o.y + (long long)c * ld + r;
+          if (o.beta != 0.0) val += o.beta * *yp;
+          *yp = val;
         }
       }
     }
@@ -916,6 +925,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_update_oz(OzuArgs u) {
     __syncthreads();
     tc_fence_after();
   }
+  cp_async_wait<0>();
   if (failed && tid == 0) atomicExch(u.err, 1);
   tc_fence_before();
   __syncthreads();
@@ -993,12 +1003,8 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
                                                                     colmax + ops[i].off);
     BDGD_CK(cudaGetLastError());
   }
-  int nsm = 148;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) {
-    cudaGetLastError();
-    nsm = 148;
-  }
   // persistent CTAs: the same count for every (output, column tile), at most one per SM
+  const int nsm = oz_sm_count(c);
   int per = nsm / u.nct;
   if (per < 1) per = 1;
   if ((long long)per > u.nrt) per = (int)u.nrt;
