@@ -131,7 +131,9 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
 // ---------------------------------------------------------------------------
 #define OZ_CHUNK 16384
 #define OZ_MAXT 48
-#define OZ_THREADS 512
+#define OZ_THREADS 512              // digit threads of the update
+#define OZ_DTHREADS 512             // digit threads of the Gram (warps 0-15)
+#define OZ_BLOCK (OZ_DTHREADS + 32) // + the Gram's MMA warp
 #define OZ_ND 7          // digits per value
 #define OZ_DMIN 5        // lowest kept diagonal t + u
 #define OZ_NDIAG 8       // kept diagonals 5..12
@@ -200,34 +202,33 @@ struct OzArgs {
   int *err;
 };
 
-// Raw FP64 stage: 32 rows of each of the tile's columns, column c at
-// c * OZ_RAW_LD bytes (272: 16-byte aligned for the 16-byte copies, and 68
-// words apart so that 8 consecutive columns fall in 8 different bank groups).
-#define OZ_RAW_LD 272
-#define OZ_RAW_A (128 * OZ_RAW_LD)
-#define OZ_RAW_STAGE (OZ_RAW_A + 64 * OZ_RAW_LD)
-#define OZ_SMEM2 (2 * OZ_RAW_STAGE + 2 * OZ_STAGE + 4096)
+// Digit stages in shared memory (MMA operands, 43008 bytes each) and the
+// per-step raw values of a digit thread, held in registers: 8 rows of its A
+// column and 4 rows of its B column.
+#define OZ_NS 4
+#define OZ_SMEM2 (OZ_NS * OZ_STAGE + 4096)
 
-// copies of rows [r, r + 32) of the tile's columns into a raw stage, by all
-// threads in 16-byte pieces (16 per column), then one commit group
-__device__ __forceinline__ void oz_issue_step(const OzTask &tk, int ia, int jb, long long r, uint8_t *raw, int tid) {
-  const int na = min(128, tk.ka - ia * 128), nb = min(64, tk.kb - jb * 64);
+struct OzRaw {
+  double2 a[4], b[2];
+};
+
+__device__ __forceinline__ void oz_load(OzRaw &x, const double *pa, const double *pb) {
+  const double2 z = make_double2(0.0, 0.0);
+  if (pa) {
+    const double2 *p = reinterpret_cast<const double2 *>(pa);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const int seg = tid + OZ_THREADS * k;
-    const int piece = seg & 15;
-    if (seg < 2048) {
-      const int c = seg >> 4;
-      if (c < na)
-        cp_async16(raw + c * OZ_RAW_LD + piece * 16, tk.a + (long long)(ia * 128 + c) * tk.lda + r + 2 * piece);
-    } else {
-      const int c = (seg - 2048) >> 4;
-      if (c < nb)
-        cp_async16(raw + OZ_RAW_A + c * OZ_RAW_LD + piece * 16,
-                   tk.b + (long long)(jb * 64 + c) * tk.ldb + r + 2 * piece);
-    }
+    for (int i = 0; i < 4; ++i) x.a[i] = __ldg(p + i);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x.a[i] = z;
   }
-  cp_async_commit();
+  if (pb) {
+    const double2 *p = reinterpret_cast<const double2 *>(pb);
+    x.b[0] = __ldg(p);
+    x.b[1] = __ldg(p + 1);
+  } else {
+    x.b[0] = x.b[1] = z;
+  }
 }
 
 // unit -> (task, tile, chunk): chunks ascending; in chunk range
@@ -266,44 +267,75 @@ __device__ __forceinline__ void oz_unit(const OzArgs &g, int unit, int &ti, int 
 // column-major, each column scaled by its maximum over all rows (pre-pass).
 // Persistent: one CTA per SM walks the work units (task, 128 x 64 output
 // tile, 16384-row chunk) chunk by chunk, so that the CTAs working at one
-// time share rows in L2.  Per unit: raw FP64 rows stream in by cp.async two
-// steps ahead; every thread turns 8 values of an A column and 4 of a B column
-// into digits; one thread issues the 34 MMAs of the step; TMEM accumulates
-// the unit; the flush writes its FP64 chunk partial.
-__global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
+// time share rows in L2.  Warp-specialised per unit:
+//  * 16 digit warps: each thread loads 8 rows of one A column and 4 rows of
+//    one B column straight into registers two steps ahead, turns them into
+//    digits and stores them into a digit stage (thread-to-column mapping
+//    chosen so that each warp's stores hit 32 distinct banks), then signals
+//    the stage;
+//  * one MMA warp: waits for each digit stage and issues its products, whose
+//    commit frees the stage.  The 34 digit products of a step are grouped by
+//    A digit t over consecutive B digits u (N = 64 per digit, up to 256): the
+//    B digits of a stage are contiguous and the accumulator of diagonal
+//    t + u sits at TMEM column 64 (t + u - 5), so one MMA with N = 64 c adds
+//    A_t [B_u .. B_u+c-1] into diagonals t + u .. t + u + c - 1 (11 MMAs per
+//    step, which cuts the operand reads from shared memory from 204 KB to
+//    112 KB).  The first step of a unit initialises each diagonal with
+//    single-digit MMAs instead.
+// TMEM accumulates the unit; the digit warps flush its FP64 chunk partial.
+__device__ __forceinline__ bool oz_wait(uint64_t *bar, uint32_t &bits, int s, volatile int *fail) {
+  const uint32_t ph = (bits >> s) & 1u;
+  bits ^= 1u << s;
+  if (*fail) return false;
+  const bool ok = mbar_wait(bar, ph, TC_WAIT_LIMIT);
+  if (!ok) *fail = 1;
+  return ok;
+}
+
+__global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  uint8_t *raw0 = oz_smem;                     // [2][OZ_RAW_STAGE]
-  uint8_t *dig0 = oz_smem + 2 * OZ_RAW_STAGE;  // [2][OZ_STAGE]
-  uint8_t *misc = dig0 + 2 * OZ_STAGE;
+  uint8_t *dig0 = oz_smem;  // [OZ_NS][OZ_STAGE]
+  uint8_t *misc = dig0 + OZ_NS * OZ_STAGE;
   double *scaleA = reinterpret_cast<double *>(misc);
   double *scaleB = scaleA + 128;
   int *SA = reinterpret_cast<int *>(scaleB + 64);
   int *SB = SA + 128;
   int *badA = SB + 64;
   int *badB = badA + 128;
-  uint64_t *mdone = reinterpret_cast<uint64_t *>(badB + 64);  // [2] MMAs of a digit stage done
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 2);
+  uint64_t *dfull = reinterpret_cast<uint64_t *>(badB + 64);  // [OZ_NS] digit stage written (16 warp arrivals)
+  uint64_t *mdone = dfull + OZ_NS;                            // [OZ_NS] MMAs of a digit stage done (commit)
+  uint64_t *fin = mdone + OZ_NS;                              // every MMA of the CTA done (exit path)
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(fin + 1);
+  volatile int *fail = reinterpret_cast<volatile int *>(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool mma_warp = warp == OZ_DTHREADS / 32;
   if (warp == 0) tmem_alloc(tslot, 512);
   if (tid == 0) {
-    for (int i = 0; i < 2; ++i) mbar_init(&mdone[i], 1);
+    for (int i = 0; i < OZ_NS; ++i) {
+      mbar_init(&dfull[i], OZ_DTHREADS / 32);
+      mbar_init(&mdone[i], 1);
+    }
+    mbar_init(fin, 1);
+    *fail = 0;
     mbar_init_fence();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  uint32_t mph[2] = {0u, 0u};
-  int failed = 0;
+  uint32_t dbits = 0u, mbits = 0u;  // mbarrier phases per stage
 
-  // digit roles: A column ca rows [8 hq, 8 hq + 8); B column cb rows [4 he, 4 he + 4)
-  const int ca = tid & 127, hq = tid >> 7;
-  const int cb = tid & 63, he = tid >> 6;
+  // digit roles (warp w, lane l): A column ca, rows [8 hq, 8 hq + 8) of the
+  // step; B column cb, rows [4 he, 4 he + 4).  Within a warp the A stores
+  // (8 bytes) of each half-warp and the B stores (4 bytes) cover one 128-byte
+  // row group of the K-major layout exactly once.
+  const int ca = (warp & 7) * 16 + ((lane >> 4) & 1) * 8 + (lane & 7), hq = ((warp >> 3) & 1) * 2 + ((lane >> 3) & 1);
+  const int cb = (warp & 7) * 8 + (lane & 7), he = ((warp >> 3) & 1) * 4 + (lane >> 3);
   const int offA = (ca & 7) * 16 + (ca >> 3) * 256 + (hq >> 1) * 128 + (hq & 1) * 8;
   const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + (he >> 2) * 128 + (he & 3) * 4;
 
-  for (int unit = blockIdx.x; unit < nunits && !failed; unit += gridDim.x) {
+  for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
     int ti, ia, jb, split;
     oz_unit(g, unit, ti, ia, jb, split);
     const OzTask &tk = g.t[ti];
@@ -315,129 +347,123 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
       const int c = ia * 128 + tid;
       double s = 1.0;
       int S = 0;
-      bool fin = true;
-      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin);
+      bool fin_ = true;
+      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin_);
       scaleA[tid] = s;
       SA[tid] = S;
-      badA[tid] = !fin;
+      badA[tid] = !fin_;
     } else if (tid < 192) {
       const int c = jb * 64 + tid - 128;
       double s = 1.0;
       int S = 0;
-      bool fin = true;
-      if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin);
+      bool fin_ = true;
+      if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin_);
       scaleB[tid - 128] = s;
       SB[tid - 128] = S;
-      badB[tid - 128] = !fin;
+      badB[tid - 128] = !fin_;
     }
     __syncthreads();
-    const bool va = ia * 128 + ca < tk.ka, vb = jb * 64 + cb < tk.kb;
-    const double sa = scaleA[ca], sb = scaleB[cb];
-    // prologue: raw stages for steps 0 and 1 (a commit group each, empty past the end)
-    for (int k = 0; k < 2; ++k) {
-      if (k < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * k, raw0 + k * OZ_RAW_STAGE, tid);
-      else cp_async_commit();
-    }
-
-    for (int ks = 0; ks < nsteps; ++ks) {
-      const int s = ks & 1;
-      uint8_t *raw = raw0 + s * OZ_RAW_STAGE;
-      uint8_t *dig = dig0 + s * OZ_STAGE;
-      cp_async_wait<1>();  // this thread's copies of step ks are done (the newest group is step ks + 1)
-      bool ok = true;
-      if (ks >= 2) {  // the MMAs of step ks - 2 read this digit stage
-        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
-        mph[s] ^= 1u;
-      }
-      failed = __syncthreads_or(!ok);
-      if (failed) break;
-      {
-        uint32_t w0[OZ_ND], w1[OZ_ND];
-        if (va) {
-          const double2 *p = reinterpret_cast<const double2 *>(raw + ca * OZ_RAW_LD + hq * 64);
-          const double2 x0 = p[0], x1 = p[1], x2 = p[2], x3 = p[3];
-          oz_digits4(x0.x, x0.y, x1.x, x1.y, sa, w0);
-          oz_digits4(x2.x, x2.y, x3.x, x3.y, sa, w1);
-        } else {
+    if (!mma_warp) {
+      const double *pa = ia * 128 + ca < tk.ka ? tk.a + (long long)(ia * 128 + ca) * tk.lda + r0 + 8 * hq : nullptr;
+      const double *pb = jb * 64 + cb < tk.kb ? tk.b + (long long)(jb * 64 + cb) * tk.ldb + r0 + 4 * he : nullptr;
+      const double sa = scaleA[ca], sb = scaleB[cb];
+      auto load = [&](OzRaw &x, int ks) { oz_load(x, pa ? pa + 32LL * ks : nullptr, pb ? pb + 32LL * ks : nullptr); };
+      auto step = [&](const OzRaw &x, int ks) {
+        const int s = ks & (OZ_NS - 1);
+        uint8_t *dig = dig0 + s * OZ_STAGE;
+        uint32_t w0[OZ_ND], w1[OZ_ND], wb[OZ_ND];
+        oz_digits4(x.a[0].x, x.a[0].y, x.a[1].x, x.a[1].y, sa, w0);
+        oz_digits4(x.a[2].x, x.a[2].y, x.a[3].x, x.a[3].y, sa, w1);
+        oz_digits4(x.b[0].x, x.b[0].y, x.b[1].x, x.b[1].y, sb, wb);
+        if (ks >= OZ_NS) oz_wait(&mdone[s], mbits, s, fail);  // the MMAs of step ks - OZ_NS read this stage
 #pragma unroll
-          for (int t = 0; t < OZ_ND; ++t) w0[t] = w1[t] = 0u;
+        for (int t = 0; t < OZ_ND; ++t) {
+          *reinterpret_cast<uint2 *>(dig + t * 4096 + offA) = make_uint2(w0[t], w1[t]);
+          *reinterpret_cast<uint32_t *>(dig + OZ_STAGE_A + t * 2048 + offB) = wb[t];
         }
-#pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint2 *>(dig + t * 4096 + offA) = make_uint2(w0[t], w1[t]);
-        if (vb) {
-          const double2 *p = reinterpret_cast<const double2 *>(raw + OZ_RAW_A + cb * OZ_RAW_LD + he * 32);
-          const double2 x0 = p[0], x1 = p[1];
-          oz_digits4(x0.x, x0.y, x1.x, x1.y, sb, w0);
-        } else {
-#pragma unroll
-          for (int t = 0; t < OZ_ND; ++t) w0[t] = 0u;
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dfull[s]);
+      };
+      OzRaw x0, x1;
+      if (nsteps > 0) load(x0, 0);
+      if (nsteps > 1) load(x1, 1);
+      for (int ks = 0; ks < nsteps; ks += 2) {
+        step(x0, ks);
+        if (ks + 2 < nsteps) load(x0, ks + 2);
+        if (ks + 1 < nsteps) {
+          step(x1, ks + 1);
+          if (ks + 3 < nsteps) load(x1, ks + 3);
         }
-#pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) *reinterpret_cast<uint32_t *>(dig + OZ_STAGE_A + t * 2048 + offB) = w0[t];
       }
-      fence_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        const uint32_t id = idesc_i8(64);
-        const uint32_t base = smem_u32(dig);
+      // the unit's accumulators are complete once the last commits arrived
+      for (int k = nsteps > OZ_NS ? nsteps - OZ_NS : 0; k < nsteps; ++k)
+        oz_wait(&mdone[k & (OZ_NS - 1)], mbits, k & (OZ_NS - 1), fail);
+    } else {
+      for (int ks = 0; ks < nsteps; ++ks) {
+        const int s = ks & (OZ_NS - 1);
+        if (lane == 0) {
+          const bool ok = oz_wait(&dfull[s], dbits, s, fail);
+          tc_fence_after();
+          const uint32_t base = smem_u32(dig0 + s * OZ_STAGE);
+          if (ok && ks == 0) {
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t)
+            for (int t = 0; t < OZ_ND; ++t)
 #pragma unroll
-          for (int u = 0; u < OZ_ND; ++u) {
-            const int D = t + u;
-            if (D < OZ_DMIN) continue;
-            const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-            mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
-                   smem_desc(base + OZ_STAGE_A + u * 2048), id, (ks > 0 || t > first_t) ? 1u : 0u);
+              for (int u = 0; u < OZ_ND; ++u) {
+                const int D = t + u;
+                if (D < OZ_DMIN) continue;
+                const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
+                mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
+                       smem_desc(base + OZ_STAGE_A + u * 2048), idesc_i8(64), t > first_t ? 1u : 0u);
+              }
+          } else if (ok) {
+#pragma unroll
+            for (int t = 0; t < OZ_ND; ++t)
+#pragma unroll
+              for (int u0 = (OZ_DMIN - t > 0 ? OZ_DMIN - t : 0); u0 < OZ_ND; u0 += 4) {
+                const int cnt = OZ_ND - u0 < 4 ? OZ_ND - u0 : 4;
+                mma_i8(tmem + (uint32_t)((t + u0 - OZ_DMIN) * 64), smem_desc(base + t * 4096),
+                       smem_desc(base + OZ_STAGE_A + u0 * 2048), idesc_i8(64 * cnt), 1u);
+              }
           }
-        mma_commit(&mdone[s]);
+          mma_commit(&mdone[s]);
+        }
+        __syncwarp();
       }
-      // the raw stage is consumed: refill it with step ks + 2
-      if (ks + 2 < nsteps) oz_issue_step(tk, ia, jb, r0 + 32LL * (ks + 2), raw, tid);
-      else cp_async_commit();
     }
-    cp_async_wait<0>();
-    if (failed) break;
-    // wait for the last commit of each digit stage used by this unit
-    if (nsteps > 0) {
-      bool ok = true;
-      for (int k = nsteps >= 2 ? nsteps - 2 : 0; k < nsteps && ok; ++k) {
-        const int s = k & 1;
-        ok = mbar_wait(&mdone[s], mph[s], TC_WAIT_LIMIT);
-        mph[s] ^= 1u;
-      }
-      failed = __syncthreads_or(!ok);
-      if (failed) break;
-    }
+    tc_fence_before();
+    __syncthreads();
     tc_fence_after();
-    // flush: warp w reads TMEM lanes 32 (w % 4).., columns 16 (w / 4)..
-    const int row = 32 * (warp & 3) + lane;
-    const int i = ia * 128 + row;
-    const long long kk = (long long)tk.ka * tk.kb;
-    double *part = g.part + tk.part0 + (long long)split * kk;
-    const int c0 = 16 * (warp >> 2);
-    double acc[16];
+    if (!mma_warp) {
+      // flush: warp w reads TMEM lanes 32 (w % 4).., columns 16 (w / 4)..
+      const int row = 32 * (warp & 3) + lane;
+      const int i = ia * 128 + row;
+      const long long kk = (long long)tk.ka * tk.kb;
+      double *part = g.part + tk.part0 + (long long)split * kk;
+      const int c0 = 16 * (warp >> 2);
+      double acc[16];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-    if (nsteps > 0) {
+      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+      if (nsteps > 0) {
 #pragma unroll
-      for (int d = 0; d < OZ_NDIAG; ++d) {
-        int32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
-        const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+        for (int d = 0; d < OZ_NDIAG; ++d) {
+          int32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
+          const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
+          for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
+        }
       }
-    }
-    if (i < tk.ka) {
+      if (i < tk.ka) {
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int j = jb * 64 + c0 + q;
-        if (j < tk.kb) {
-          double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
-          if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
-          part[(long long)j * tk.ka + i] = val;
+        for (int q = 0; q < 16; ++q) {
+          const int j = jb * 64 + c0 + q;
+          if (j < tk.kb) {
+            double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
+            if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
+            part[(long long)j * tk.ka + i] = val;
+          }
         }
       }
     }
@@ -445,10 +471,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_gram_oz(OzArgs g, long long c
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    if (*fail) break;
   }
-  if (failed && tid == 0) atomicExch(g.err, 1);
+  // MMAs still in flight after a timeout end before TMEM is freed
+  if (mma_warp && lane == 0) {
+    mma_commit(fin);
+    if (!mbar_wait(fin, 0, TC_WAIT_LIMIT)) *fail = 1;
+  }
   tc_fence_before();
   __syncthreads();
+  if (*fail && tid == 0) atomicExch(g.err, 1);
   if (warp == 0) tmem_free(tmem, 512);
 }
 
@@ -617,7 +649,7 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
   if (!bdgd_capturing)
     BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM2));
   bdgd_count_launch();
-  k_gram_oz<<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_THREADS, OZ_SMEM2, c->stream>>>(g, chunk, nunits);
+  k_gram_oz<<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_BLOCK, OZ_SMEM2, c->stream>>>(g, chunk, nunits);
   BDGD_CK(cudaGetLastError());
   bdgd_count_launch();
   k_oz_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, ldo, d_out);
