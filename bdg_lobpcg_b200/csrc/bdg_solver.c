@@ -928,6 +928,11 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
   int use_learned = bdg->learned != NULL && !w->cplx && bdg->learned_fallback < 0;
   const int stall_win = bdg->learned_stall > 0 ? bdg->learned_stall : 12;
   double hist[256];
+  /* BDG_P_SVQB=1: SVQB-normalise the projected P as well (one more Gram,
+   * eigen-decomposition and two GEMMs per iteration; same iteration count on
+   * the 128^3 benchmark solve, 6% slower) */
+  const char *psv = getenv("BDG_P_SVQB");
+  const int p_svqb = psv ? psv[0] == '1' : 0;
   for (;;) {
     cudaEventRecord(w->ev[3], st);
     TRY(measure(w, dev, o->anorm, lam, back, tres, want_true));
@@ -1006,18 +1011,25 @@ static int run_loop(ws_t *w, bdgd_ctx *dev, bdg_t *bdg, const loop_opts_t *o, do
         upd_term(&o[1], B(NB_AX), m, w->Cs, m);
         TRY(bupdate(w, dev, 0, 2, o));
       }
-      t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 1, 0, 0, 1, 0);
-      DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
-      TRY(svqb(w, dev, w->gout + (size_t)K * K * es, p, K, drop, w->Cs, &pk));
-      /* Cs holds Z_P (p x pk, leading dim p) */
-      {
-        bdgd_update_out o[2] = {upd_out(B(NB_T1), pk, 1.0, 0.0), upd_out(B(NB_T2), pk, 1.0, 0.0)};
-        upd_term(&o[0], B(NB_P), p, w->Cs, p);
-        upd_term(&o[1], B(NB_AP), p, w->Cs, p);
-        TRY(bupdate(w, dev, 0, 2, o));
+      if (p_svqb) {
+        t[0] = mk_task(w, B(NB_P), B(NB_P), w->n, p, p, 1, 0, 0, 1, 0);
+        DEV_TRY(bdgd_gram_tasks(dev, w->prec, w->cplx, 1, t, K, w->gout));
+        TRY(svqb(w, dev, w->gout + (size_t)K * K * es, p, K, drop, w->Cs, &pk));
+        /* Cs holds Z_P (p x pk, leading dim p) */
+        {
+          bdgd_update_out o[2] = {upd_out(B(NB_T1), pk, 1.0, 0.0), upd_out(B(NB_T2), pk, 1.0, 0.0)};
+          upd_term(&o[0], B(NB_P), p, w->Cs, p);
+          upd_term(&o[1], B(NB_AP), p, w->Cs, p);
+          TRY(bupdate(w, dev, 0, 2, o));
+        }
+        swapb(w, NB_P, NB_T1);
+        swapb(w, NB_AP, NB_T2);
+      } else {
+        /* the projected P enters [X, P] as it is: the W projection's
+         * pseudo-inverse and the Rayleigh-Ritz step's scaled eigen-
+         * decomposition drop its dependent directions */
+        pk = p;
       }
-      swapb(w, NB_P, NB_T1);
-      swapb(w, NB_AP, NB_T2);
     }
     /* W <- (Wt - Q (Q^H Q)^+ Q^H Wt) Z_W, Q = [X, P] */
     const int q = m + pk;

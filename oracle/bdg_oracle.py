@@ -667,14 +667,14 @@ def svqb_coeffs(G, drop=1e-13):
 
 def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
             criterion=CONV_BACKWARD, lock=True, drop=1e-13, guard=1e-4, guard_strict=1e-12, stall_win=10,
-            project_p=True, verbose=False):
+            project_p=True, normalize_p=False, verbose=False):
     """Block iLOBPCG for the pencil (A, B) = (diag(K, M), swap).
 
     X0: (m, n) block (rows are the columns of the reference's S), B-positive.
     Per iteration (the GPU solver runs the same steps):
       R = A X - B X diag(lam) on the active columns, W = T R
-      (project_p only: P <- P - X (X^H X)^+ X^H P, then SVQB-normalised,
-      AP transformed alike)
+      (project_p only: P <- P - X (X^H X)^+ X^H P, AP alike; SVQB-normalised
+      as well only with normalize_p)
       W <- W - Q (Q^H Q)^+ Q^H W with Q = [X, P], then SVQB-normalised
       Rayleigh-Ritz on S = [X, P, W]  (rr_pencil)
       X <- S C,  P <- [P, W] C_pw  (restricted to the active columns)
@@ -689,7 +689,11 @@ def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
     P is re-projected against X and SVQB-normalised each iteration
     (project_p).  Without it the small cases converge alike (16^3 42 / 42,
     32^3 78 / 78 iterations), but on the GPU the 128^3 FP64 solve stalled at a
-    true residual of 1.2e-8 for 4 of 32 pairs, so the projection stays."""
+    true residual of 1.2e-8 for 4 of 32 pairs, so the projection stays.  Its
+    SVQB normalisation does not: the W projection's pseudo-inverse and the
+    Rayleigh-Ritz step's scaled eigen-decomposition drop the dependent
+    directions of the projected P (32^3 78 / 78, 64^3 65 / 66 iterations with
+    and without it, eigenvalues to 5e-15; 128^3 on the GPU 63 / 63)."""
     A = applyA or (lambda Z: matmulLrep(ctx, Z))
     T = applyT or (lambda Z: precondLrep(ctx, Z))
     anorm = anorm_estimate(ctx)
@@ -736,9 +740,10 @@ def ilobpcg(ctx, X0, nev, maxIter, tol, proj=None, applyA=None, applyT=None,
             Cpx = gram_pinv(X.conj() @ X.T, drop) @ (X.conj() @ P.T)
             P = P - Cpx.T @ X
             AP = AP - Cpx.T @ AX
-            Z = svqb_coeffs(P.conj() @ P.T, drop)
-            P = Z.T @ P
-            AP = Z.T @ AP
+            if normalize_p:
+                Z = svqb_coeffs(P.conj() @ P.T, drop)
+                P = Z.T @ P
+                AP = Z.T @ AP
         Q = X if P is None else np.concatenate([X, P])
         Y = gram_pinv(Q.conj() @ Q.T, drop) @ (Q.conj() @ W.T)
         W = W - Y.T @ Q

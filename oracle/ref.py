@@ -74,6 +74,7 @@ def lib():
         "ref_helper_anorm": (f64, [vp]),
         "ilobpcg_shim_set": (None, [i32, i32, i32, f64, f64, i32, f64]),
         "ilobpcg_shim_threads": (None, [i32]),
+        "ilobpcg_shim_set_pnorm": (None, [i32]),
         "ilobpcg_shim_timeline": (i32, [C.POINTER(f64), i32, C.POINTER(i32), C.POINTER(i32)]),
         "ilobpcg_shim_history": (i32, [i32, i32, C.POINTER(f64), C.POINTER(f64)]),
         "ilobpcg_shim_capture_init": (None, [vp]),
@@ -183,9 +184,10 @@ class RefProblem:
         return out
 
     def solve(self, criterion=CONV_BACKWARD, deflate=False, lock=True, guard=1e-4, guard_strict=1e-12,
-              stall_win=10, true_gate=1e-7):
+              stall_win=10, true_gate=1e-7, normalize_p=False):
         self.L_.ilobpcg_shim_set(int(criterion), 1 if deflate else 0, 1 if lock else 0, guard, guard_strict,
                                  stall_win, true_gate)
+        self.L_.ilobpcg_shim_set_pnorm(1 if normalize_p else 0)
         rc = self.L_.bdg_solve(self.h)
         if rc != 0:
             raise RuntimeError(f"bdg_solve (oracle build) returned {rc}")

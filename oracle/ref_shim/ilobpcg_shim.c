@@ -54,9 +54,10 @@ typedef struct {
   int deflate;
   int stall_win;
   double drop, guard, guard_strict, true_gate;
+  int norm_p; /* SVQB-normalise the projected P (off: as the GPU solver) */
 } shim_opts_t;
 
-static shim_opts_t g_opt = {0, 1, 0, 10, 1e-13, 1e-4, 1e-12, 1e-7};
+static shim_opts_t g_opt = {0, 1, 0, 10, 1e-13, 1e-4, 1e-12, 1e-7, 0};
 
 /* Capture mode: the next solve copies the initial block that the caller's
  * init switch wrote into alg->S (src/solver.c:167-259) to this buffer and
@@ -75,6 +76,8 @@ void ilobpcg_shim_set(int criterion, int deflate, int lock, double guard, double
   g_opt.stall_win = stall_win > 0 && stall_win < 64 ? stall_win : 10;
   g_opt.true_gate = true_gate;
 }
+
+void ilobpcg_shim_set_pnorm(int on) { g_opt.norm_p = on != 0; }
 
 void ilobpcg_shim_threads(int nthreads) {
   scipy_openblas_set_num_threads(nthreads);
