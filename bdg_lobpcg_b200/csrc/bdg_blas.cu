@@ -681,20 +681,23 @@ __global__ void k_gram_tasks_reduce(GArgs g, int cplx, int ldo, double *__restri
   }
 }
 
-extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out);
+extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out);
+#define BDG_GRAM_TC_F32_DEFAULT 0
 
-// Tensor-core (int8 digits, tcgen05) FP64 Gram for real FP64 blocks: on with
-// BDG_GRAM_TC=1
-static bool gram_tc_on() {
+// Tensor-core (int8 digits, tcgen05) Gram for real FP64 or FP32 blocks:
+// BDG_GRAM_TC=1 turns it on for both, BDG_GRAM_TC=0 off for both; unset, it
+// serves the FP32 blocks (faster than DMMA there) and not the FP64 ones
+static bool gram_tc_on(int prec) {
   const char *e = getenv("BDG_GRAM_TC");
-  return e && e[0] == '1';
+  if (e && e[0]) return e[0] == '1';
+  return prec == BDGD_F32 && BDG_GRAM_TC_F32_DEFAULT;
 }
 
 extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const bdgd_gram_task *tasks, int ldo,
                                double *d_out) {
   if (ntask <= 0) return BDGD_OK;
-  if (prec == BDGD_F64 && !cplx && gram_tc_on()) {
-    const int rc = bdgd_gram_oz(c, ntask, tasks, ldo, d_out);
+  if ((prec == BDGD_F64 || prec == BDGD_F32) && !cplx && gram_tc_on(prec)) {
+    const int rc = bdgd_gram_oz(c, prec, ntask, tasks, ldo, d_out);
     if (rc != BDGD_ERR_UNSUPPORTED) return rc;
   }
   if (ntask > GMAXT) {

@@ -142,7 +142,10 @@ extern "C" int bdgd_tc_i8_gemm(void *stream, const int8_t *A, uint64_t lda, cons
 #define OZ_STAGE_B (OZ_ND * 64 * 32)
 #define OZ_STAGE (OZ_STAGE_A + OZ_STAGE_B)
 
-__device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale, int &S, bool &finite) {
+// scale = 2^(P - S) with 2^(S - 1) above the column's largest |x|, the
+// exponent clamped to [pmin, pmax] (the scale's own range)
+__device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale, int &S, bool &finite, int P = OZ_P,
+                                         int pmin = -1022, int pmax = 1023) {
   const double m = __longlong_as_double((long long)bits);
   finite = isfinite(m);
   if (!(m > 0.0) || !finite) {  // zero column (or not finite: flagged at the flush)
@@ -153,9 +156,9 @@ __device__ __forceinline__ void oz_scale(unsigned long long bits, double &scale,
   int E = 0;
   frexp(m, &E);  // m = f 2^E, f in [0.5, 1): |x| < 2^E
   S = E + 1;
-  int p = OZ_P - S;
-  if (p > 1023) p = 1023;
-  if (p < -1022) p = -1022;
+  int p = P - S;
+  if (p > pmax) p = pmax;
+  if (p < pmin) p = pmin;
   scale = ldexp(1.0, p);
 }
 
@@ -184,8 +187,40 @@ __device__ __forceinline__ void oz_digits4(double v0, double v1, double v2, doub
   w[6] = __byte_perm(b2, b3, 0x5410);
 }
 
+// FP32 values (the FP32 phase of the mixed form): X = rint(x 2^(31 - S)),
+// |X| < 2^30, in 4 signed 8-bit digits from the bytes of X + 0x808080;
+// w[t] holds digit t of the four values
+__device__ __forceinline__ void oz_digits4f(float v0, float v1, float v2, float v3, float scale,
+                                            uint32_t (&w)[4]) {
+  uint32_t lo[4];
+  const float v[4] = {v0, v1, v2, v3};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) lo[q] = (uint32_t)(__float2int_rn(v[q] * scale) + 0x808080) ^ 0x808080u;
+  const uint32_t a0 = __byte_perm(lo[0], lo[1], 0x5140), a1 = __byte_perm(lo[2], lo[3], 0x5140);
+  const uint32_t a2 = __byte_perm(lo[0], lo[1], 0x7362), a3 = __byte_perm(lo[2], lo[3], 0x7362);
+  w[0] = __byte_perm(a0, a1, 0x5410);
+  w[1] = __byte_perm(a0, a1, 0x7632);
+  w[2] = __byte_perm(a2, a3, 0x5410);
+  w[3] = __byte_perm(a2, a3, 0x7632);
+}
+
+// digit formats of the Gram per input type: digits per value, lowest kept
+// diagonal, kept diagonals, fixed-point bits, range of the scale exponent
+template <typename T>
+struct OzFmt;
+template <>
+struct OzFmt<double> {
+  static constexpr int ND = 7, DMIN = 5, NDIAG = 8, P = 55, PMIN = -1022, PMAX = 1023;
+};
+template <>
+struct OzFmt<float> {
+  // diagonals t + u >= 2 of 4 x 4 (13 products); the dropped ones are below
+  // 2^-33 of max|a| max|b| per term, under the FP32 inputs' own rounding
+  static constexpr int ND = 4, DMIN = 2, NDIAG = 5, P = 31, PMIN = -126, PMAX = 127;
+};
+
 struct OzTask {
-  const double *a, *b;
+  const void *a, *b;
   long long lda, ldb, rows;
   int ka, kb, out, i0, j0, sym, mirror;
   int ta, tb, ntile, tile0;
@@ -202,17 +237,54 @@ struct OzArgs {
   int *err;
 };
 
-// Digit stages in shared memory (MMA operands, 43008 bytes each) and the
-// per-step raw values of a digit thread, held in registers: 8 rows of its A
-// column and 4 rows of its B column.
+// Digit stages in shared memory (MMA operands, 6144 bytes per digit: 43008
+// for FP64 values, 24576 for FP32) and the per-step raw values of a digit
+// thread, held in registers: 8 rows of its A column and 4 rows of its B
+// column.
 #define OZ_NS 4
-#define OZ_SMEM2 (OZ_NS * OZ_STAGE + 4096)
+template <typename T>
+constexpr int oz_smem_bytes() {
+  return OZ_NS * OzFmt<T>::ND * 6144 + 4096;
+}
 
-struct OzRaw {
+template <typename T>
+struct OzRaw;
+template <>
+struct OzRaw<double> {
   double2 a[4], b[2];
 };
+template <>
+struct OzRaw<float> {
+  float4 a[2], b;
+};
 
-__device__ __forceinline__ void oz_load(OzRaw &x, const double *pa, const double *pb) {
+__device__ __forceinline__ void oz_load(OzRaw<float> &x, const float *pa, const float *pb) {
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (pa) {
+    const float4 *p = reinterpret_cast<const float4 *>(pa);
+    x.a[0] = __ldg(p);
+    x.a[1] = __ldg(p + 1);
+  } else {
+    x.a[0] = x.a[1] = z;
+  }
+  x.b = pb ? __ldg(reinterpret_cast<const float4 *>(pb)) : z;
+}
+
+// the step's digits of a digit thread: w0 / w1 the A rows 0-3 / 4-7, wb the B rows
+__device__ __forceinline__ void oz_step_digits(const OzRaw<double> &x, double sa, double sb, uint32_t (&w0)[7],
+                                               uint32_t (&w1)[7], uint32_t (&wb)[7]) {
+  oz_digits4(x.a[0].x, x.a[0].y, x.a[1].x, x.a[1].y, sa, w0);
+  oz_digits4(x.a[2].x, x.a[2].y, x.a[3].x, x.a[3].y, sa, w1);
+  oz_digits4(x.b[0].x, x.b[0].y, x.b[1].x, x.b[1].y, sb, wb);
+}
+__device__ __forceinline__ void oz_step_digits(const OzRaw<float> &x, double sa, double sb, uint32_t (&w0)[4],
+                                               uint32_t (&w1)[4], uint32_t (&wb)[4]) {
+  oz_digits4f(x.a[0].x, x.a[0].y, x.a[0].z, x.a[0].w, (float)sa, w0);
+  oz_digits4f(x.a[1].x, x.a[1].y, x.a[1].z, x.a[1].w, (float)sa, w1);
+  oz_digits4f(x.b.x, x.b.y, x.b.z, x.b.w, (float)sb, wb);
+}
+
+__device__ __forceinline__ void oz_load(OzRaw<double> &x, const double *pa, const double *pb) {
   const double2 z = make_double2(0.0, 0.0);
   if (pa) {
     const double2 *p = reinterpret_cast<const double2 *>(pa);
@@ -292,10 +364,13 @@ __device__ __forceinline__ bool oz_wait(uint64_t *bar, uint32_t &bits, int s, vo
   return ok;
 }
 
+template <typename T>
 __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chunk, int nunits) {
+  constexpr int ND = OzFmt<T>::ND, DMIN = OzFmt<T>::DMIN, NDIAG = OzFmt<T>::NDIAG, P = OzFmt<T>::P;
+  constexpr int STAGE_A = ND * 4096, STAGE = ND * 6144;  // A: 128 x 32 bytes, B: 64 x 32 bytes per digit
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  uint8_t *dig0 = oz_smem;  // [OZ_NS][OZ_STAGE]
-  uint8_t *misc = dig0 + OZ_NS * OZ_STAGE;
+  uint8_t *dig0 = oz_smem;  // [OZ_NS][STAGE]
+  uint8_t *misc = dig0 + OZ_NS * STAGE;
   double *scaleA = reinterpret_cast<double *>(misc);
   double *scaleB = scaleA + 128;
   int *SA = reinterpret_cast<int *>(scaleB + 64);
@@ -348,7 +423,7 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
       double s = 1.0;
       int S = 0;
       bool fin_ = true;
-      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin_);
+      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin_, P, OzFmt<T>::PMIN, OzFmt<T>::PMAX);
       scaleA[tid] = s;
       SA[tid] = S;
       badA[tid] = !fin_;
@@ -357,35 +432,34 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
       double s = 1.0;
       int S = 0;
       bool fin_ = true;
-      if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin_);
+      if (c < tk.kb) oz_scale(g.colmax[tk.mb + c], s, S, fin_, P, OzFmt<T>::PMIN, OzFmt<T>::PMAX);
       scaleB[tid - 128] = s;
       SB[tid - 128] = S;
       badB[tid - 128] = !fin_;
     }
     __syncthreads();
     if (!mma_warp) {
-      const double *pa = ia * 128 + ca < tk.ka ? tk.a + (long long)(ia * 128 + ca) * tk.lda + r0 + 8 * hq : nullptr;
-      const double *pb = jb * 64 + cb < tk.kb ? tk.b + (long long)(jb * 64 + cb) * tk.ldb + r0 + 4 * he : nullptr;
+      const T *ta = static_cast<const T *>(tk.a), *tb = static_cast<const T *>(tk.b);
+      const T *pa = ia * 128 + ca < tk.ka ? ta + (long long)(ia * 128 + ca) * tk.lda + r0 + 8 * hq : nullptr;
+      const T *pb = jb * 64 + cb < tk.kb ? tb + (long long)(jb * 64 + cb) * tk.ldb + r0 + 4 * he : nullptr;
       const double sa = scaleA[ca], sb = scaleB[cb];
-      auto load = [&](OzRaw &x, int ks) { oz_load(x, pa ? pa + 32LL * ks : nullptr, pb ? pb + 32LL * ks : nullptr); };
-      auto step = [&](const OzRaw &x, int ks) {
+      auto load = [&](OzRaw<T> &x, int ks) { oz_load(x, pa ? pa + 32LL * ks : nullptr, pb ? pb + 32LL * ks : nullptr); };
+      auto step = [&](const OzRaw<T> &x, int ks) {
         const int s = ks & (OZ_NS - 1);
-        uint8_t *dig = dig0 + s * OZ_STAGE;
-        uint32_t w0[OZ_ND], w1[OZ_ND], wb[OZ_ND];
-        oz_digits4(x.a[0].x, x.a[0].y, x.a[1].x, x.a[1].y, sa, w0);
-        oz_digits4(x.a[2].x, x.a[2].y, x.a[3].x, x.a[3].y, sa, w1);
-        oz_digits4(x.b[0].x, x.b[0].y, x.b[1].x, x.b[1].y, sb, wb);
+        uint8_t *dig = dig0 + s * STAGE;
+        uint32_t w0[ND], w1[ND], wb[ND];
+        oz_step_digits(x, sa, sb, w0, w1, wb);
         if (ks >= OZ_NS) oz_wait(&mdone[s], mbits, s, fail);  // the MMAs of step ks - OZ_NS read this stage
 #pragma unroll
-        for (int t = 0; t < OZ_ND; ++t) {
+        for (int t = 0; t < ND; ++t) {
           *reinterpret_cast<uint2 *>(dig + t * 4096 + offA) = make_uint2(w0[t], w1[t]);
-          *reinterpret_cast<uint32_t *>(dig + OZ_STAGE_A + t * 2048 + offB) = wb[t];
+          *reinterpret_cast<uint32_t *>(dig + STAGE_A + t * 2048 + offB) = wb[t];
         }
         fence_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(&dfull[s]);
       };
-      OzRaw x0, x1;
+      OzRaw<T> x0, x1;
       if (nsteps > 0) load(x0, 0);
       if (nsteps > 1) load(x1, 1);
       for (int ks = 0; ks < nsteps; ks += 2) {
@@ -405,26 +479,26 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
         if (lane == 0) {
           const bool ok = oz_wait(&dfull[s], dbits, s, fail);
           tc_fence_after();
-          const uint32_t base = smem_u32(dig0 + s * OZ_STAGE);
+          const uint32_t base = smem_u32(dig0 + s * STAGE);
           if (ok && ks == 0) {
 #pragma unroll
-            for (int t = 0; t < OZ_ND; ++t)
+            for (int t = 0; t < ND; ++t)
 #pragma unroll
-              for (int u = 0; u < OZ_ND; ++u) {
+              for (int u = 0; u < ND; ++u) {
                 const int D = t + u;
-                if (D < OZ_DMIN) continue;
-                const int first_t = D - (OZ_ND - 1) > 0 ? D - (OZ_ND - 1) : 0;
-                mma_i8(tmem + (uint32_t)((D - OZ_DMIN) * 64), smem_desc(base + t * 4096),
-                       smem_desc(base + OZ_STAGE_A + u * 2048), idesc_i8(64), t > first_t ? 1u : 0u);
+                if (D < DMIN) continue;
+                const int first_t = D - (ND - 1) > 0 ? D - (ND - 1) : 0;
+                mma_i8(tmem + (uint32_t)((D - DMIN) * 64), smem_desc(base + t * 4096),
+                       smem_desc(base + STAGE_A + u * 2048), idesc_i8(64), t > first_t ? 1u : 0u);
               }
           } else if (ok) {
 #pragma unroll
-            for (int t = 0; t < OZ_ND; ++t)
+            for (int t = 0; t < ND; ++t)
 #pragma unroll
-              for (int u0 = (OZ_DMIN - t > 0 ? OZ_DMIN - t : 0); u0 < OZ_ND; u0 += 4) {
-                const int cnt = OZ_ND - u0 < 4 ? OZ_ND - u0 : 4;
-                mma_i8(tmem + (uint32_t)((t + u0 - OZ_DMIN) * 64), smem_desc(base + t * 4096),
-                       smem_desc(base + OZ_STAGE_A + u0 * 2048), idesc_i8(64 * cnt), 1u);
+              for (int u0 = (DMIN - t > 0 ? DMIN - t : 0); u0 < ND; u0 += 4) {
+                const int cnt = ND - u0 < 4 ? ND - u0 : 4;
+                mma_i8(tmem + (uint32_t)((t + u0 - DMIN) * 64), smem_desc(base + t * 4096),
+                       smem_desc(base + STAGE_A + u0 * 2048), idesc_i8(64 * cnt), 1u);
               }
           }
           mma_commit(&mdone[s]);
@@ -447,10 +521,10 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
       for (int q = 0; q < 16; ++q) acc[q] = 0.0;
       if (nsteps > 0) {
 #pragma unroll
-        for (int d = 0; d < OZ_NDIAG; ++d) {
+        for (int d = 0; d < NDIAG; ++d) {
           int32_t v[16];
           tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c0), v);
-          const double w = ldexp(1.0, 8 * (d + OZ_DMIN) - 2 * OZ_P);
+          const double w = ldexp(1.0, 8 * (d + DMIN) - 2 * P);
 #pragma unroll
           for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
         }
@@ -486,14 +560,15 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
 
 // |x| maxima of the columns of an operand (FP64 bit patterns, atomic max;
 // the target starts at zero)
-__global__ void k_oz_colmax(const double *__restrict__ a, long long lda, long long rows, long long span,
+template <typename T>
+__global__ void k_oz_colmax(const T *__restrict__ a, long long lda, long long rows, long long span,
                             unsigned long long *__restrict__ out) {
   const int c = blockIdx.x;
   const long long rb = (long long)blockIdx.y * span, re = min(rows, rb + span);
-  const double *col = a + (long long)c * lda;
+  const T *col = a + (long long)c * lda;
   double m = 0.0;
   for (long long r = rb + threadIdx.x; r < re; r += blockDim.x) {
-    const double x = fabs(__ldg(col + r));
+    const double x = fabs((double)__ldg(col + r));
     m = (x > m || x != x) ? x : m;  // NaN propagates
   }
   __shared__ double red[32];
@@ -541,13 +616,26 @@ static int oz_sm_count(bdgd_ctx *c) {
 
 // Real FP64 task list on the tensor cores; BDGD_ERR_UNSUPPORTED (nothing
 // launched) for layouts outside the kernel's limits.
-extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out) {
+template <typename T>
+static int gram_oz_launch(bdgd_ctx *c, const OzArgs &g, long long chunk, int nunits, int nsm) {
+  if (!bdgd_capturing)
+    BDGD_CK(cudaFuncSetAttribute(k_gram_oz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz_smem_bytes<T>()));
+  bdgd_count_launch();
+  k_gram_oz<T><<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_BLOCK, oz_smem_bytes<T>(), c->stream>>>(g, chunk, nunits);
+  BDGD_CK(cudaGetLastError());
+  return BDGD_OK;
+}
+
+// prec: BDGD_F64 (FP64 blocks) or BDGD_F32 (FP32 blocks, FP64 results)
+extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out) {
   if (ntask <= 0) return BDGD_OK;
-  if (ntask > OZ_MAXT) return BDGD_ERR_UNSUPPORTED;
+  if (ntask > OZ_MAXT || (prec != BDGD_F64 && prec != BDGD_F32)) return BDGD_ERR_UNSUPPORTED;
+  const uint64_t vec = prec == BDGD_F64 ? 2 : 4;  // elements per 16 bytes
   long long maxrows = 0;
   for (int i = 0; i < ntask; ++i) {
     const bdgd_gram_task &s = tasks[i];
-    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % 2 || s.ldb % 2 || s.ka <= 0 || s.kb <= 0 || s.rows % 32)
+    if (((uintptr_t)s.a | (uintptr_t)s.b) % 16 || s.lda % vec || s.ldb % vec || s.ka <= 0 || s.kb <= 0 ||
+        s.rows % 32)
       return BDGD_ERR_UNSUPPORTED;
     if ((long long)s.rows > maxrows) maxrows = (long long)s.rows;
   }
@@ -565,7 +653,7 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     }
   // unique operands (pointer, leading dimension, rows, columns) -> column maxima
   struct Op {
-    const double *p;
+    const void *p;
     long long ld, rows;
     int k, off;
   } ops[2 * OZ_MAXT];
@@ -574,7 +662,7 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     for (int i = 0; i < nops; ++i)
       if (ops[i].p == p && ops[i].ld == (long long)ld && ops[i].rows == (long long)rows && ops[i].k == k)
         return ops[i].off;
-    ops[nops] = {(const double *)p, (long long)ld, (long long)rows, k, moff};
+    ops[nops] = {p, (long long)ld, (long long)rows, k, moff};
     moff += k;
     return ops[nops++].off;
   };
@@ -582,8 +670,8 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
   for (int q = 0; q < ntask; ++q) {
     const bdgd_gram_task &s = tasks[order[q]];
     OzTask &t = g.t[q];
-    t.a = (const double *)s.a;
-    t.b = (const double *)s.b;
+    t.a = s.a;
+    t.b = s.b;
     t.lda = (long long)s.lda;
     t.ldb = (long long)s.ldb;
     t.rows = (long long)s.rows;
@@ -642,15 +730,18 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int ntask, const bdgd_gram_task *tasks,
     const long long span = 65536;
     const unsigned ny = (unsigned)((ops[i].rows + span - 1) / span);
     bdgd_count_launch();
-    k_oz_colmax<<<dim3((unsigned)ops[i].k, ny ? ny : 1), 256, 0, c->stream>>>(ops[i].p, ops[i].ld, ops[i].rows, span,
-                                                                             colmax + ops[i].off);
+    const dim3 grid((unsigned)ops[i].k, ny ? ny : 1);
+    if (prec == BDGD_F64)
+      k_oz_colmax<double><<<grid, 256, 0, c->stream>>>((const double *)ops[i].p, ops[i].ld, ops[i].rows, span,
+                                                       colmax + ops[i].off);
+    else
+      k_oz_colmax<float><<<grid, 256, 0, c->stream>>>((const float *)ops[i].p, ops[i].ld, ops[i].rows, span,
+                                                      colmax + ops[i].off);
     BDGD_CK(cudaGetLastError());
   }
-  if (!bdgd_capturing)
-    BDGD_CK(cudaFuncSetAttribute(k_gram_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM2));
-  bdgd_count_launch();
-  k_gram_oz<<<(unsigned)(nunits < nsm ? nunits : nsm), OZ_BLOCK, OZ_SMEM2, c->stream>>>(g, chunk, nunits);
-  BDGD_CK(cudaGetLastError());
+  rc = prec == BDGD_F64 ? gram_oz_launch<double>(c, g, chunk, nunits, nsm)
+                        : gram_oz_launch<float>(c, g, chunk, nunits, nsm);
+  if (rc) return rc;
   bdgd_count_launch();
   k_oz_reduce<<<dim3(32, ntask), 256, 0, c->stream>>>(g, ldo, d_out);
   BDGD_CK(cudaGetLastError());
@@ -1031,7 +1122,7 @@ extern "C" int bdgd_block_update_oz(bdgd_ctx *c, uint64_t n, uint64_t ld, int no
     const long long span = 65536;
     const unsigned ny = (unsigned)(((long long)n + span - 1) / span);
     bdgd_count_launch();
-    k_oz_colmax<<<dim3((unsigned)ops[i].k, ny), 256, 0, c->stream>>>(ops[i].p, (long long)ld, (long long)n, span,
+    k_oz_colmax<double><<<dim3((unsigned)ops[i].k, ny), 256, 0, c->stream>>>(ops[i].p, (long long)ld, (long long)n, span,
                                                                     colmax + ops[i].off);
     BDGD_CK(cudaGetLastError());
   }

@@ -96,9 +96,48 @@ def test_gram_tc_matches_reference(bdg, monkeypatch, rows, k, kind):
     dc.close()
 
 
-@pytest.mark.parametrize("fixture,nev", [("gs16", 4), ("c1_32", 8)])
-def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
-    """The whole solve with the tensor-core Gram and update: same eigenvalues
+@pytest.mark.parametrize("rows,k,kind", [(4096, 64, "random"), (40000, 70, "weighted"), (262144, 192, "random"),
+                                         (131072, 130, "weighted")])
+def test_gram_tc_fp32_matches_reference(bdg, monkeypatch, rows, k, kind):
+    """The tensor-core Gram of FP32 blocks (4 int8 digits per value, the FP32
+    phase of the mixed form) against the exact FP64 product of the same FP32
+    values: |G - G_ref| <= 2^-30 (max|a_i| sum|b_j| + max|b_j| sum|a_i|),
+    twice the bound of its 31-bit fixed-point rounding (the DMMA kernel,
+    which widens the values to FP64, is held to 1e-14 of the same scale)."""
+    torch = _torch()
+    X, AX = _gram_blocks(torch, rows, k, rows + 3 * k, kind)
+    X, AX = X.float(), AX.float()
+    n = 2 * rows
+    dc = bdg.DeviceContext(3, [16, 16, 16], [8.0] * 3, False)
+    outs = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("BDG_GRAM_TC", mode)
+        out = torch.full((4 * k * k,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        dc.gram_ptr(1, False, rows, k, X.data_ptr(), n, AX.data_ptr(), n, out.data_ptr())
+        dc.synchronize()
+        outs[mode] = out.cpu().numpy().reshape(4, k, k)
+    x = X.cpu().numpy().astype(np.float64)
+    ax = AX.cpu().numpy().astype(np.float64)
+    xu, xv = x[:, :rows], x[:, rows:]
+    pairs = [(xu, xu), (xv, xv), (xu, xv), (x, ax)]
+    for q, (a, b) in enumerate(pairs):
+        ref = a @ b.T
+        ma, mb = np.abs(a).max(axis=1), np.abs(b).max(axis=1)
+        sa, sb = np.abs(a).sum(axis=1), np.abs(b).sum(axis=1)
+        scale = np.maximum(np.outer(ma, sb) + np.outer(sa, mb), 1e-300)
+        for mode, tol in (("0", 1e-14), ("1", 2.0 ** -30)):
+            got = outs[mode][q].T
+            assert np.all(np.isfinite(got)), (mode, q)
+            err = float((np.abs(got - ref) / scale).max())
+            assert err < tol, (mode, q, err)
+    dc.close()
+
+
+@pytest.mark.parametrize("fixture,nev,prec", [("gs16", 4, "f64"), ("c1_32", 8, "f64"), ("c1_32", 8, "mixed")])
+def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev, prec):
+    """The whole solve with the tensor-core Gram and update (FP64, or the
+    mixed form with its FP32-phase Gram on the tensor cores): same eigenvalues
     as with the DMMA kernels (1e-12 relative) and the true residual <= tol."""
     import os
 
@@ -127,6 +166,7 @@ def test_solve_with_tc_gram_matches_dmma(bdg, monkeypatch, fixture, nev):
         p.set_initial_block(X0)
         p.set_goldstone_deflation(True)
         p.set_convergence(bdg.CONV_TRUE_RESIDUAL)
+        p.set_precision(bdg.PREC_MIXED if prec == "mixed" else bdg.PREC_F64)
         assert p.solve() == 0 and p.converged() >= nev
         st = p.stats()
         assert st["max_true_residual"] <= tol
