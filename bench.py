@@ -526,6 +526,82 @@ def kernel_main(argv):
     return {"ops": kernel_ops, "gram": kernel_gram, "update": kernel_update}[a.kernel](a)
 
 
+def c3_config():
+    """The complex (_z) configuration: 128^3 in [-12, 12)^3, lambda 1, g 1500,
+    eps_dd 0.4, R_c 8, nev 48 (sizeSub 96), tol 1e-8 on the true residual,
+    complex N(0, 1) initial block (v = u) at seed 2."""
+    g = 1500.0
+    return dict(N=[128] * 3, L=[24.0] * 3, omegas=(1.0, 1.0, 1.0), g=g, gdd=0.4 * g, eps_dd=0.4, lam=1.0, rc=8.0,
+                nev=48, sizeSub=96, tol=1e-8, seed=2)
+
+
+def run_c3(args):
+    """--config c3: the complex path at 128^3, complex128 and complex64 with
+    FP64 refinement, on psi0 = e^{0.7 i} psi_real (a genuinely complex
+    condensate; the fixed-winding vortex of this physics makes K = H - mu
+    indefinite, outside the definite-pencil iLOBPCG), Goldstone chain
+    deflated.  Prints one JSON line with both forms."""
+    import bdg_lobpcg_b200 as B
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if not B.gpu_available():
+        raise RuntimeError("bench needs a CUDA device")
+    cfg = c3_config()
+    psi, mu, itp_steps, stationarity, V = ground_state(B, cfg)
+    psi_z = psi * np.exp(0.7j)
+    size = int(np.prod(cfg["N"]))
+    rng = np.random.default_rng(cfg["seed"])
+    u = rng.standard_normal((cfg["sizeSub"], size)) + 1j * rng.standard_normal((cfg["sizeSub"], size))
+    X0 = np.concatenate([u, u], axis=1)
+    forms = {}
+    for prec in ("f64", "mixed"):
+        p = B.Problem(3, cfg["N"], cfg["L"], complex_psi0=True)
+        p.set_system()
+        p.set_trap(V)
+        p.set_wavefunction(psi_z)
+        g = cfg["g"]
+        p.set_local_interactions(lambda n: g * n, lambda n: g * n)
+        p.set_dipolar(cfg["gdd"], [0.0, 0.0, 1.0], cfg["rc"])
+        p.set_mu(mu)
+        p.set_solver_params(cfg["nev"], cfg["sizeSub"], 2000, cfg["tol"])
+        p.set_convergence(B.CONV_TRUE_RESIDUAL)
+        p.set_goldstone_deflation(True)
+        p.set_precision(B.PREC_MIXED if prec == "mixed" else B.PREC_F64)
+        p.set_initial_block(X0)
+        for _ in range(args.warmup):
+            if p.solve():
+                raise RuntimeError("bdg_solve (complex) failed")
+        dev, e2e = [], []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            if p.solve():
+                raise RuntimeError("bdg_solve (complex) failed")
+            e2e.append(time.perf_counter() - t)
+            dev.append(p.stats()["seconds_device"])
+        st = p.stats()
+        forms[prec] = {"value": float(np.mean(dev)), "e2e": float(np.mean(e2e)), "unit": "s",
+                       "iterations": st["iterations"], "refine_iterations": st["refine_iterations"],
+                       "converged": p.converged(), "max_true_residual": st["max_true_residual"],
+                       "eigenvalues": [float(v) for v in p.eigenvalues()],
+                       "stage_ms": {k: st[k] for k in ("ms_apply_A", "ms_apply_T", "ms_residual", "ms_gram",
+                                                        "ms_small_dense", "ms_update")}}
+        p.close()
+    ef = np.asarray(forms["f64"]["eigenvalues"])
+    em = np.asarray(forms["mixed"]["eigenvalues"])
+    line = {"metric": "time to res<=1e-8, 48 BdG modes @128^3, complex path", "value": forms["f64"]["value"],
+            "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "complex BdG 128^3 dipolar trap (eps_dd 0.4, lambda 1, g 1500), psi0 = "
+                                   "e^{0.7i} psi_real, nev 48, sizeSub 96, tol 1e-8 true residual, deflated",
+                       "grid": cfg["N"], "nev": cfg["nev"], "sizeSub": cfg["sizeSub"]},
+            "ground_state": {"mu": mu, "itp_steps": itp_steps, "stationarity": stationarity},
+            "complex128": forms["f64"], "complex64_fp64": forms["mixed"],
+            "eig_rel_err_mixed_vs_c128": float(np.max(np.abs(em - ef) / np.abs(ef)))}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     if "--kernel" in sys.argv[1:]:
         return kernel_main(sys.argv[1:])
@@ -536,6 +612,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c3"],
+                    help="c2: the 128^3 real headline; c3: the complex path (own JSON line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-iters", type=int, default=1,
                     help="whole reference-path iterations timed for cpu_baseline")
@@ -545,6 +623,8 @@ def main():
     cfg = problem_config(args.grid)
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.config == "c3":
+        return run_c3(args)
 
     import bdg_lobpcg_b200 as B
 
