@@ -186,6 +186,13 @@ template <> struct GStage<float, true> { typedef float2 E; static constexpr int 
 template <typename T, bool CPLX, int V> struct GStageV : GStage<T, CPLX> {};
 template <typename T> struct GStageV<T, false, 1> { typedef typename GStage<T, false>::E E; static constexpr int RK = 16, LDE = 20; };
 template <typename T> struct GStageV<T, true, 1> { typedef typename GStage<T, true>::E E; static constexpr int RK = 8, LDE = 10; };
+// V = 3 (real, BDG_GRAM_VARIANT=3): a ring of three 16-row stages with one
+// barrier per stage, the loads two stages ahead of the DMMA work (60 KB,
+// three blocks per SM).  At 128^3, k = 192: 24.0 against 24.6 ms for V = 1;
+// four-stage rings (8 rows at four blocks per SM, 16 rows at two) measured
+// 36.4 and 25.8 ms.
+template <typename T> struct GStageV<T, false, 3> { typedef typename GStage<T, false>::E E; static constexpr int RK = 16, LDE = 20; };
+template <int V> constexpr int gram_nstage() { return V == 3 ? 3 : 2; }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -400,24 +407,51 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
   const T *A = (const T *)tk.a;
   const T *B = (const T *)tk.b;
   const long long nst = rend > rbeg ? (rend - rbeg + RK - 1) / RK : 0;
-  if (nst > 0) {
+  constexpr int NS = gram_nstage<V>();
+  if constexpr (NS > 2) {
+    // ring of NS stages: stages 0 .. NS-2 in flight before the first; one
+    // (possibly empty) commit group per stage keeps the wait counts uniform
+#pragma unroll
+    for (int q = 0; q < NS - 1; ++q) {
+      if (q < nst) {
+        E *st = buf + q * 2 * GT * LDE;
+        stage_async<T, CPLX, V>(st, A, tk.lda, ti * GT, tk.ka, rbeg + q * RK, rend);
+        stage_async<T, CPLX, V>(st + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg + q * RK, rend);
+      }
+      cp_async_commit();
+    }
+  } else if (nst > 0) {
     stage_async<T, CPLX, V>(buf, A, tk.lda, ti * GT, tk.ka, rbeg, rend);
     stage_async<T, CPLX, V>(buf + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg, rend);
     cp_async_commit();
   }
   for (long long s = 0; s < nst; ++s) {
-    E *cur = buf + (s & 1) * 2 * GT * LDE;
-    if (s + 1 < nst) {
-      E *nxt = buf + ((s + 1) & 1) * 2 * GT * LDE;
-      const long long r0 = rbeg + (s + 1) * RK;
-      stage_async<T, CPLX, V>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
-      stage_async<T, CPLX, V>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
+    E *cur;
+    if constexpr (NS > 2) {
+      cur = buf + (int)(s % NS) * 2 * GT * LDE;
+      cp_async_wait<NS - 2>();  // this thread's copies of stage s have landed
+      __syncthreads();          // everyone's, and stage s - 1 is consumed by all warps
+      const long long q = s + NS - 1;
+      if (q < nst) {
+        E *st = buf + (int)(q % NS) * 2 * GT * LDE;
+        stage_async<T, CPLX, V>(st, A, tk.lda, ti * GT, tk.ka, rbeg + q * RK, rend);
+        stage_async<T, CPLX, V>(st + GT * LDE, B, tk.ldb, tj * GT, tk.kb, rbeg + q * RK, rend);
+      }
       cp_async_commit();
-      cp_async_wait<1>();
     } else {
-      cp_async_wait<0>();
+      cur = buf + (s & 1) * 2 * GT * LDE;
+      if (s + 1 < nst) {
+        E *nxt = buf + ((s + 1) & 1) * 2 * GT * LDE;
+        const long long r0 = rbeg + (s + 1) * RK;
+        stage_async<T, CPLX, V>(nxt, A, tk.lda, ti * GT, tk.ka, r0, rend);
+        stage_async<T, CPLX, V>(nxt + GT * LDE, B, tk.ldb, tj * GT, tk.kb, r0, rend);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const E *sA = cur, *sB = cur + GT * LDE;
 #pragma unroll
     for (int kk = 0; kk < RK; kk += 4) {
@@ -469,6 +503,11 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
         }
       }
     }
+    if constexpr (NS == 2) __syncthreads();
+  }
+  if constexpr (NS > 2) {
+    // the next segment's prologue refills the ring: every warp done with it
+    cp_async_wait<0>();
     __syncthreads();
   }
 #pragma unroll
@@ -492,9 +531,10 @@ __device__ __forceinline__ void gram_tile_rows(const GTask &tk, int ti, int tj, 
 // threads per block of a k_gram_sk variant (V = 2 splits real and imaginary
 // accumulation over twice the warps)
 template <int V> constexpr int gram_threads() { return V == 2 ? 256 : 128; }
+template <int V> constexpr int gram_min_blocks() { return V == 1 ? 4 : V == 3 ? 3 : V == 2 ? 2 : 1; }
 
 template <typename T, bool CPLX, int V>
-__global__ void __launch_bounds__(gram_threads<V>(), V == 1 ? 4 : (V == 2 ? 2 : 1)) k_gram_sk(GArgsSK g) {
+__global__ void __launch_bounds__(gram_threads<V>(), gram_min_blocks<V>()) k_gram_sk(GArgsSK g) {
   typedef typename GStageV<T, CPLX, V>::E E;
   constexpr int ES = CPLX ? 2 : 1;
   extern __shared__ __align__(16) unsigned char gsm3[];
@@ -587,7 +627,7 @@ static int launch_gram_sk(bdgd_ctx *c, const GArgs &ga, int cplx, int ldo, doubl
   typedef typename GStageV<T, CPLX, V>::E E;
   const int es = cplx ? 2 : 1;
   if (ga.ntiles > GMAXTILES) return BDGD_ERR_UNSUPPORTED;
-  const size_t sm = sizeof(E) * 2 * 2 * GT * GStageV<T, CPLX, V>::LDE;
+  const size_t sm = sizeof(E) * gram_nstage<V>() * 2 * GT * GStageV<T, CPLX, V>::LDE;
   if (sm > 48 * 1024)
     BDGD_CK(cudaFuncSetAttribute(k_gram_sk<T, CPLX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   static thread_local GArgsSK g;  // large; host-side staging of the kernel parameters
@@ -766,12 +806,14 @@ extern "C" int bdgd_gram_tasks(bdgd_ctx *c, int prec, int cplx, int ntask, const
     // the full-height stages at three blocks per SM)
     const char *gv = getenv("BDG_GRAM_VARIANT");
     const bool half = !(gv && gv[0] == '0');
+    const int ring = gv ? atoi(gv) : 0;  // 3: the three-stage ring (real FP64)
     // complex FP64: real and imaginary parts on separate warps (29.8 against
     // 28.9 TF/s at 128^3, k = 192; in FP32 the one-warp form is faster)
     if (prec == BDGD_F32) rc = cplx ? launch_gram_sk<float, true, 0>(c, g, cplx, ldo, d_out)
                                     : launch_gram_sk<float, false, 0>(c, g, cplx, ldo, d_out);
     else if (cplx) rc = half ? launch_gram_sk<double, true, 2>(c, g, cplx, ldo, d_out)
                              : launch_gram_sk<double, true, 0>(c, g, cplx, ldo, d_out);
+    else if (ring == 3) rc = launch_gram_sk<double, false, 3>(c, g, cplx, ldo, d_out);
     else rc = half ? launch_gram_sk<double, false, 1>(c, g, cplx, ldo, d_out)
                    : launch_gram_sk<double, false, 0>(c, g, cplx, ldo, d_out);
     if (rc != BDGD_ERR_UNSUPPORTED) return rc;
