@@ -223,15 +223,24 @@ struct OzTask {
   const void *a, *b;
   long long lda, ldb, rows;
   int ka, kb, out, i0, j0, sym, mirror;
-  int ta, tb, ntile, tile0;
   int nsp;                // row chunks of this task
   int ma, mb;             // offsets of the operands' column maxima
   long long part0;        // offset of the task's chunk partials (doubles)
 };
 
+// A 128 x 64 output tile: two 64-column slices of A operands (of one task or
+// of two tasks that share the B operand, its rows and its columns) against
+// one 64-column tile of B, so that tasks of 64 columns fill whole tiles.
+struct OzTile {
+  short ta[2], sa[2];     // task and 64-column slice of each half (ta = -1: empty)
+  short tb, jb;           // task of the B operand and rows, B column tile
+  int nsp;                // row chunks
+};
+#define OZ_MAXTILES 640
 struct OzArgs {
-  OzTask t[OZ_MAXT];      // sorted by nsp, largest first
-  int nt, ntiles;
+  OzTask t[OZ_MAXT];
+  OzTile p[OZ_MAXTILES];  // sorted by nsp, largest first
+  int nt, np;
   const unsigned long long *colmax;  // |x| maxima as FP64 bit patterns
   double *part;
   int *err;
@@ -303,32 +312,17 @@ __device__ __forceinline__ void oz_load(OzRaw<double> &x, const double *pa, cons
   }
 }
 
-// unit -> (task, tile, chunk): chunks ascending; in chunk range
-// [nsp_{i+1}, nsp_i) the tasks 0..i (sorted by nsp, largest first) are active
-__device__ __forceinline__ void oz_unit(const OzArgs &g, int unit, int &ti, int &ia, int &jb, int &split) {
+// unit -> (tile, chunk): chunks ascending; in chunk range [nsp_{i+1},
+// nsp_i) the tiles 0..i (sorted by nsp, largest first) are active
+__device__ __forceinline__ void oz_unit(const OzArgs &g, int unit, int &tile, int &split) {
   int u = unit;
-  ti = 0;
-  ia = jb = split = 0;
-  for (int i = g.nt - 1; i >= 0; --i) {
-    const int lo = (i == g.nt - 1) ? 0 : g.t[i + 1].nsp, hi = g.t[i].nsp;
-    const int P = g.t[i].tile0 + g.t[i].ntile;  // tiles of tasks 0..i
-    const int cnt = (hi - lo) * P;
+  tile = split = 0;
+  for (int i = g.np - 1; i >= 0; --i) {
+    const int lo = (i == g.np - 1) ? 0 : g.p[i + 1].nsp, hi = g.p[i].nsp;
+    const int cnt = (hi - lo) * (i + 1);
     if (u < cnt) {
-      split = lo + u / P;
-      const int gt = u - (u / P) * P;
-      while (ti + 1 <= i && g.t[ti + 1].tile0 <= gt) ++ti;
-      const OzTask &tk = g.t[ti];
-      int lt = gt - tk.tile0;
-      if (tk.sym) {  // tiles with 2 ia <= jb only (the rest comes from the transpose)
-        while (lt >= tk.tb - 2 * ia) {
-          lt -= tk.tb - 2 * ia;
-          ++ia;
-        }
-        jb = 2 * ia + lt;
-      } else {
-        ia = lt / tk.tb;
-        jb = lt - ia * tk.tb;
-      }
+      split = lo + u / (i + 1);
+      tile = u - (u / (i + 1)) * (i + 1);
       return;
     }
     u -= cnt;
@@ -411,19 +405,23 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
   const int offB = (cb & 7) * 16 + (cb >> 3) * 256 + (he >> 2) * 128 + (he & 3) * 4;
 
   for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
-    int ti, ia, jb, split;
-    oz_unit(g, unit, ti, ia, jb, split);
-    const OzTask &tk = g.t[ti];
+    int pt, split;
+    oz_unit(g, unit, pt, split);
+    const OzTile tile = g.p[pt];
+    const OzTask &tk = g.t[tile.tb];  // the B operand and the row range
+    const int jb = tile.jb;
     const long long r0 = (long long)split * chunk;
     const long long r1 = min(tk.rows, r0 + chunk);
     const int nsteps = r1 > r0 ? (int)((r1 - r0) / 32) : 0;  // rows are a multiple of 32
 
     if (tid < 128) {
-      const int c = ia * 128 + tid;
+      // A column tid: half tid / 64 of the tile, column 64 sa + tid % 64 of its task
+      const int h = tid >> 6, tA = tile.ta[h];
+      const int c = tile.sa[h] * 64 + (tid & 63);
       double s = 1.0;
       int S = 0;
       bool fin_ = true;
-      if (c < tk.ka) oz_scale(g.colmax[tk.ma + c], s, S, fin_, P, OzFmt<T>::PMIN, OzFmt<T>::PMAX);
+      if (tA >= 0 && c < g.t[tA].ka) oz_scale(g.colmax[g.t[tA].ma + c], s, S, fin_, P, OzFmt<T>::PMIN, OzFmt<T>::PMAX);
       scaleA[tid] = s;
       SA[tid] = S;
       badA[tid] = !fin_;
@@ -439,9 +437,13 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
     }
     __syncthreads();
     if (!mma_warp) {
-      const T *ta = static_cast<const T *>(tk.a), *tb = static_cast<const T *>(tk.b);
-      const T *pa = ia * 128 + ca < tk.ka ? ta + (long long)(ia * 128 + ca) * tk.lda + r0 + 8 * hq : nullptr;
-      const T *pb = jb * 64 + cb < tk.kb ? tb + (long long)(jb * 64 + cb) * tk.ldb + r0 + 4 * he : nullptr;
+      const int tA = tile.ta[ca >> 6], colA = tile.sa[ca >> 6] * 64 + (ca & 63);
+      const T *pa = nullptr;
+      if (tA >= 0 && colA < g.t[tA].ka)
+        pa = static_cast<const T *>(g.t[tA].a) + (long long)colA * g.t[tA].lda + r0 + 8 * hq;
+      const T *pb = jb * 64 + cb < tk.kb
+                        ? static_cast<const T *>(tk.b) + (long long)(jb * 64 + cb) * tk.ldb + r0 + 4 * he
+                        : nullptr;
       const double sa = scaleA[ca], sb = scaleB[cb];
       auto load = [&](OzRaw<T> &x, int ks) { oz_load(x, pa ? pa + 32LL * ks : nullptr, pb ? pb + 32LL * ks : nullptr); };
       auto step = [&](const OzRaw<T> &x, int ks) {
@@ -512,9 +514,11 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
     if (!mma_warp) {
       // flush: warp w reads TMEM lanes 32 (w % 4).., columns 16 (w / 4)..
       const int row = 32 * (warp & 3) + lane;
-      const int i = ia * 128 + row;
-      const long long kk = (long long)tk.ka * tk.kb;
-      double *part = g.part + tk.part0 + (long long)split * kk;
+      const int tA = tile.ta[row >> 6];
+      const OzTask &to = g.t[tA >= 0 ? tA : tile.tb];  // the task this row's output belongs to
+      const int i = tile.sa[row >> 6] * 64 + (row & 63);
+      const long long kk = (long long)to.ka * to.kb;
+      double *part = g.part + to.part0 + (long long)split * kk;
       const int c0 = 16 * (warp >> 2);
       double acc[16];
 #pragma unroll
@@ -529,14 +533,14 @@ __global__ void __launch_bounds__(OZ_BLOCK, 1) k_gram_oz(OzArgs g, long long chu
           for (int q = 0; q < 16; ++q) acc[q] = fma((double)v[q], w, acc[q]);
         }
       }
-      if (i < tk.ka) {
+      if (tA >= 0 && i < to.ka) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const int j = jb * 64 + c0 + q;
-          if (j < tk.kb) {
+          if (j < to.kb) {
             double val = ldexp(acc[q], SA[row] + SB[c0 + q]);
             if (badA[row] || badB[c0 + q]) val = __longlong_as_double(0x7ff8000000000000LL);
-            part[(long long)j * tk.ka + i] = val;
+            part[(long long)j * to.ka + i] = val;
           }
         }
       }
@@ -592,7 +596,7 @@ __global__ void k_oz_reduce(OzArgs g, int ldo, double *__restrict__ outbuf) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < kk; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % tk.ka), j = (int)(q / tk.ka);
     int si = i, sj = j;
-    if (tk.sym && 2 * (i / 128) > j / 64) {
+    if (tk.sym && i / 64 > j / 64) {  // below the computed 64 x 64 blocks: the transpose
       si = j;
       sj = i;
     }
@@ -666,7 +670,6 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_ta
     moff += k;
     return ops[nops++].off;
   };
-  int tiles = 0;
   for (int q = 0; q < ntask; ++q) {
     const bdgd_gram_task &s = tasks[order[q]];
     OzTask &t = g.t[q];
@@ -680,22 +683,56 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_ta
     t.out = s.out;
     t.i0 = s.i0;
     t.j0 = s.j0;
-    t.sym = s.sym && s.ka == s.kb;  // a symmetric result: upper tiles computed
+    t.sym = s.sym && s.ka == s.kb;  // a symmetric result: the 64 x 64 blocks on and above the diagonal
     t.mirror = s.mirror;
-    t.ta = (s.ka + 127) / 128;
-    t.tb = (s.kb + 63) / 64;
-    if (t.sym) {
-      t.ntile = 0;
-      for (int a = 0; a < t.ta; ++a) t.ntile += t.tb - 2 * a > 0 ? t.tb - 2 * a : 0;
-    } else {
-      t.ntile = t.ta * t.tb;
-    }
-    t.tile0 = tiles;
-    tiles += t.ntile;
     t.ma = op_index(s.a, s.lda, s.rows, s.ka);
     t.mb = op_index(s.b, s.ldb, s.rows, s.kb);
   }
-  g.ntiles = tiles;
+  // 64 x 64 output blocks (task, A slice, B tile), grouped by B operand and B
+  // tile (operands are identified by their column-maxima slot, which is
+  // unique per pointer, leading dimension, rows and columns); consecutive
+  // blocks of a group share one 128 x 64 tile
+  struct Blk {
+    int t, s, jb, key;
+  };
+  static thread_local Blk blk[OZ_MAXTILES * 2];
+  int nblk = 0;
+  for (int q = 0; q < ntask; ++q) {
+    const OzTask &t = g.t[q];
+    const int sa = (t.ka + 63) / 64, tb = (t.kb + 63) / 64;
+    for (int jb = 0; jb < tb; ++jb)
+      for (int sl = 0; sl < sa; ++sl) {
+        if (t.sym && sl > jb) continue;
+        if (nblk >= OZ_MAXTILES * 2) return BDGD_ERR_UNSUPPORTED;
+        blk[nblk++] = {q, sl, jb, t.mb * 1024 + jb};
+      }
+  }
+  // stable order by key (tasks already in order of decreasing rows)
+  for (int i = 1; i < nblk; ++i)
+    for (int j = i; j > 0 && blk[j].key < blk[j - 1].key; --j) {
+      const Blk x = blk[j];
+      blk[j] = blk[j - 1];
+      blk[j - 1] = x;
+    }
+  int tiles = 0;
+  for (int i = 0; i < nblk;) {
+    if (tiles >= OZ_MAXTILES) return BDGD_ERR_UNSUPPORTED;
+    OzTile &p = g.p[tiles++];
+    p.ta[0] = (short)blk[i].t;
+    p.sa[0] = (short)blk[i].s;
+    p.tb = (short)blk[i].t;
+    p.jb = (short)blk[i].jb;
+    if (i + 1 < nblk && blk[i + 1].key == blk[i].key) {
+      p.ta[1] = (short)blk[i + 1].t;
+      p.sa[1] = (short)blk[i + 1].s;
+      i += 2;
+    } else {
+      p.ta[1] = -1;
+      p.sa[1] = 0;
+      i += 1;
+    }
+  }
+  g.np = tiles;
   // row chunks: at most OZ_CHUNK rows (int32 exactness), enough units to fill the GPU
   const int nsm = oz_sm_count(c);
   long long nsplit = (2LL * nsm + tiles - 1) / tiles;
@@ -707,14 +744,24 @@ extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_ta
   long long chunk = (maxrows + nsplit - 1) / nsplit;
   chunk = (chunk + 31) / 32 * 32;
   long long off = 0;
-  int nunits = 0;
   for (int q = 0; q < ntask; ++q) {
     OzTask &t = g.t[q];
     t.nsp = (int)((t.rows + chunk - 1) / chunk);
     t.part0 = off;
     off += (long long)t.nsp * t.ka * t.kb;
-    nunits += t.nsp * t.ntile;
   }
+  int nunits = 0;
+  for (int i = 0; i < tiles; ++i) {
+    g.p[i].nsp = g.t[g.p[i].tb].nsp;
+    nunits += g.p[i].nsp;
+  }
+  // tiles in order of decreasing chunk count (stable)
+  for (int i = 1; i < tiles; ++i)
+    for (int j = i; j > 0 && g.p[j].nsp > g.p[j - 1].nsp; --j) {
+      const OzTile x = g.p[j];
+      g.p[j] = g.p[j - 1];
+      g.p[j - 1] = x;
+    }
   int rc = bdgd_ensure(c->stream, (void **)&c->gram_part, &c->gram_part_bytes, sizeof(double) * off);
   if (rc) return rc;
   // oz_buf: the error flag (16 bytes), then the column maxima
