@@ -722,7 +722,7 @@ __global__ void k_gram_tasks_reduce(GArgs g, int cplx, int ldo, double *__restri
 }
 
 extern "C" int bdgd_gram_oz(bdgd_ctx *c, int prec, int ntask, const bdgd_gram_task *tasks, int ldo, double *d_out);
-#define BDG_GRAM_TC_F32_DEFAULT 1  // 13.9 against 21.9 ms at 128^3, k = 192; mixed solve 3.30 against 3.48 s
+#define BDG_GRAM_TC_F32_DEFAULT 1  // 13.9 against 21.9 ms at 128^3, k = 192; mixed solve 3.34 against 3.49 s
 
 // Tensor-core (int8 digits, tcgen05) Gram for real FP64 or FP32 blocks:
 // BDG_GRAM_TC=1 turns it on for both, BDG_GRAM_TC=0 off for both; unset, it

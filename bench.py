@@ -678,7 +678,7 @@ def main():
     if not args.no_variants and args.precision == "f64":
         # the mixed FP32/FP64 form of the same solve (same psi0, X0), timed the same way
         pm, _ = build(B, cfg, psi, mu, V, "mixed")
-        for _ in range(min(args.warmup, 1)):
+        for _ in range(args.warmup):
             pm.solve()
         mt, me = [], []
         for _ in range(args.steps):
