@@ -36,8 +36,10 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 #include <math.h>
+#include <pthread.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
 
 #include "bdg/bdg_cuda.h"
 #include "bdg/bdg_learn.h"
@@ -130,10 +132,55 @@ static void ws_free(ws_t *w) {
   memset(w, 0, sizeof *w);
 }
 
+/* memcpy of a large host range by several threads: one thread copies at a
+ * fraction of the host memory bandwidth (about 8 GB/s), so the pageable
+ * <-> pinned copies of the 2 GB blocks of a 128^3 solve would take longer
+ * than their DMA */
+typedef struct {
+  char *dst;
+  const char *src;
+  size_t len;
+} pcopy_t;
+
+static void *pcopy_run(void *a) {
+  const pcopy_t *c = (const pcopy_t *)a;
+  memcpy(c->dst, c->src, c->len);
+  return NULL;
+}
+
+static void par_memcpy(void *dst, const void *src, size_t len) {
+  enum { MAXT = 8 };
+  long nc = sysconf(_SC_NPROCESSORS_ONLN);
+  int nt = nc > MAXT ? MAXT : (nc < 1 ? 1 : (int)nc);
+  if (len < ((size_t)8 << 20) || nt < 2) {
+    memcpy(dst, src, len);
+    return;
+  }
+  pthread_t th[MAXT];
+  pcopy_t part[MAXT];
+  int started[MAXT] = {0};
+  const size_t per = ((len + (size_t)nt - 1) / (size_t)nt + 4095) & ~(size_t)4095;
+  for (int i = 0; i < nt; i++) {
+    const size_t off = (size_t)i * per;
+    part[i].dst = (char *)dst + off;
+    part[i].src = (const char *)src + off;
+    part[i].len = off >= len ? 0 : (len - off < per ? len - off : per);
+  }
+  for (int i = 1; i < nt; i++)
+    if (part[i].len) started[i] = pthread_create(&th[i], NULL, pcopy_run, &part[i]) == 0;
+  pcopy_run(&part[0]);
+  for (int i = 1; i < nt; i++) {
+    if (started[i])
+      pthread_join(th[i], NULL);
+    else if (part[i].len)
+      pcopy_run(&part[i]); /* no thread: copy it here */
+  }
+}
+
 /* Host <-> device copy of pageable user memory through two pinned staging
  * buffers: the DMA of one chunk overlaps the host memcpy of the next
  * (pageable copies run at a fraction of the pinned rate). */
-#define PIN_BYTES ((size_t)32 << 20)
+#define PIN_BYTES ((size_t)64 << 20)
 static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2d) {
   for (int i = 0; i < 2; i++) {
     if (!w->pin[i] && cudaMallocHost(&w->pin[i], PIN_BYTES) != cudaSuccess) {
@@ -154,7 +201,7 @@ static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2
     const size_t off = i * PIN_BYTES, len = (bytes - off) < PIN_BYTES ? (bytes - off) : PIN_BYTES;
     if (h2d) {
       if (i >= 2 && cudaEventSynchronize(w->pin_ev[b]) != cudaSuccess) return -3;
-      memcpy(w->pin[b], (const char *)src + off, len);
+      par_memcpy(w->pin[b], (const char *)src + off, len);
       if (cudaMemcpyAsync((char *)dst + off, w->pin[b], len, cudaMemcpyHostToDevice, w->st) != cudaSuccess) return -3;
       cudaEventRecord(w->pin_ev[b], w->st);
     } else {
@@ -165,7 +212,7 @@ static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2
         const int pb = b ^ 1;
         const size_t poff = off - PIN_BYTES;
         if (cudaEventSynchronize(w->pin_ev[pb]) != cudaSuccess) return -3;
-        memcpy((char *)dst + poff, w->pin[pb], PIN_BYTES);
+        par_memcpy((char *)dst + poff, w->pin[pb], PIN_BYTES);
       }
     }
   }
@@ -173,7 +220,7 @@ static int staged_copy(ws_t *w, void *dst, const void *src, size_t bytes, int h2
     const int lb = (int)((nch - 1) & 1);
     const size_t loff = (nch - 1) * PIN_BYTES;
     if (cudaEventSynchronize(w->pin_ev[lb]) != cudaSuccess) return -3;
-    memcpy((char *)dst + loff, w->pin[lb], bytes - loff);
+    par_memcpy((char *)dst + loff, w->pin[lb], bytes - loff);
   }
   if (h2d && nch > 0) { /* the staging buffers are reused: wait for the last copies */
     for (int i = 0; i < 2; i++)
@@ -276,13 +323,13 @@ static int staged_d2h_segments(ws_t *w, int nseg, void *const *dst, const void *
     cudaEventRecord(w->pin_ev[b], w->st);
     if (i >= 1) {
       if (cudaEventSynchronize(w->pin_ev[b ^ 1]) != cudaSuccess) return -3;
-      memcpy(dst[i - 1], w->pin[b ^ 1], len[i - 1]);
+      par_memcpy(dst[i - 1], w->pin[b ^ 1], len[i - 1]);
     }
   }
   if (nseg > 0) {
     const int lb = (nseg - 1) & 1;
     if (cudaEventSynchronize(w->pin_ev[lb]) != cudaSuccess) return -3;
-    memcpy(dst[nseg - 1], w->pin[lb], len[nseg - 1]);
+    par_memcpy(dst[nseg - 1], w->pin[lb], len[nseg - 1]);
   }
   return 0;
 }
@@ -1216,7 +1263,27 @@ static int solve_gpu(bdg_t *bdg) {
       w->hX0_bytes = xb;
     }
   }
-  if (host_init) {
+  /* the block of bdg_set_initial_block (a host array the library borrows):
+   * copied chunk by chunk into the pinned buffer by several threads, each
+   * chunk's DMA overlapping the copy of the next */
+  const int borrowed = host_init && bdg->init_mode == BDG_INIT_CUSTOM && bdg->init_block && w->hX0 &&
+                       bdg->init_block_n == n && bdg->init_block_m == m;
+  if (borrowed) {
+    void *dst = w->blk[NB_X];
+    void *tmp = NULL;
+    if (mixed) {
+      if ((rc = dmalloc(w, &tmp, xb))) return rc;
+      dst = tmp;
+    }
+    for (size_t off = 0; off < xb; off += PIN_BYTES) {
+      const size_t len = xb - off < PIN_BYTES ? xb - off : PIN_BYTES;
+      par_memcpy((char *)w->hX0 + off, (const char *)bdg->init_block + off, len);
+      CUDA_TRY(cudaMemcpyAsync((char *)dst + off, (const char *)w->hX0 + off, len, cudaMemcpyHostToDevice, st));
+    }
+    if (mixed) DEV_TRY(bdgd_convert(dev, 1, tmp, w->blk[NB_X], n * m * (cplx ? 2 : 1)));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (tmp) dfree(w, tmp);
+  } else if (host_init) {
     const int pinned = w->hX0 != NULL;
     void *X0 = pinned ? w->hX0 : xmalloc(xb);
     /* a custom init fills every entry; the other modes rely on a zeroed block */
