@@ -212,7 +212,9 @@ int bdgd_init_block(bdgd_ctx *ctx, int prec, int mode, uint32_t seed, int ncols,
  * capture.  Every call reuses the same array: calls that may run at the same
  * time on the GPU (other streams, other host threads) race on it and must
  * be serialised by the caller.  Each call writes every partial it reads, so
- * nothing left over from an earlier call is used. */
+ * nothing left over from an earlier call is used.  The looked-up address is
+ * kept per device ordinal for the primary context: after cudaDeviceReset,
+ * or from a context other than the primary one, do not call it again. */
 int bdgd_gram_noalloc(void *stream, int prec, int cplx, uint64_t half, uint64_t k, const void *d_S, uint64_t lds,
                       const void *d_AS, uint64_t ldas, double *d_out);
 

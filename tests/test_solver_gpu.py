@@ -54,6 +54,22 @@ def test_bdg_1d_uniform_z_matches_d(bdg):
     assert abs(d[np.argmin(np.abs(d - E1))] - z[np.argmin(np.abs(z - E1))]) < 1e-4
 
 
+def test_stale_initial_block_is_refused(bdg):
+    """A block given to bdg_set_initial_block no longer fits once sizeSub
+    changes: bdg_solve returns -9 instead of starting from a zero block; a
+    block of the new shape is accepted again."""
+    p = _uniform_1d(bdg, False)
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((10, 64))
+    p.set_initial_block(np.concatenate([u, u], axis=1))
+    p.set_solver_params(4, 12, 200, 1e-4)
+    assert p.solve() == -9
+    u = rng.standard_normal((12, 64))
+    p.set_initial_block(np.concatenate([u, u], axis=1))
+    assert p.solve() == 0
+    p.close()
+
+
 @pytest.mark.parametrize("N", [32, 64])
 def test_bdg_3d_harmonic(N, bdg):
     """tests/test_bdg_3d_harmonic.c:51-108 (64^3, L=10, nev 10, sizeSub 20,
