@@ -166,3 +166,27 @@ def test_oracle_goldstone_deflation_complex_psi0():
         assert r.converged >= 4
         ev.append(r.eigvals[:4])
     assert np.all(np.abs(ev[0] - ev[1]) / ev[0] < 1e-13)
+
+
+def test_oracle_p_normalisation_does_not_change_the_solve():
+    """The projected P enters [X, P] without its own SVQB (the default of all
+    three restatements): same eigenvalues (1e-12) and iteration count within
+    one of the normalised variant on the 16^3 dipolar problem."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_fixtures as FX
+
+    fx = FX.load("gs16")
+    N = [int(v) for v in fx["N"]]
+    L = [float(v) for v in fx["L"]]
+    om = [float(v) for v in fx["omegas"]]
+    oc = O.build_problem(N, L, om, float(fx["g"]), float(fx["gdd"]), fx["psi"], float(fx["mu"]), Rc=float(fx["rc"]))
+    proj, _ = O.goldstone_projector(oc)
+    X0 = O.gaussian_block_bpositive(oc, 8, 0)
+    runs = [O.ilobpcg(oc, X0, 4, 400, 1e-8, proj=proj, criterion=O.CONV_TRUE_RESIDUAL, normalize_p=norm)
+            for norm in (True, False)]
+    assert all(r.converged >= 4 for r in runs)
+    assert np.all(np.abs(runs[0].eigvals[:4] - runs[1].eigvals[:4]) / runs[0].eigvals[:4] < 1e-12)
+    assert abs(runs[0].iters - runs[1].iters) <= 1, (runs[0].iters, runs[1].iters)
