@@ -163,6 +163,33 @@ def reference_solve_sample(cfg, psi, mu, V, X0, iters, threads):
     return res["timeline"], res
 
 
+def reference_anchor_64(threads):
+    """A whole reference-path solve timed to tolerance, no projection: the
+    64^3 configuration (nev 16, sizeSub 32, true residual <= 1e-8, Goldstone
+    chain deflated, X0 ~ N(0, 1) with v = u at seed 1) on the committed
+    stationary psi0 of that physics (tests/golden/c2_64.npz, from the
+    oracle's ground-state producer).  Returns the line's `anchor_64`."""
+    from oracle import ref as R
+
+    f = np.load(os.path.join(ROOT, "tests", "golden", "c2_64.npz"))
+    cfg = problem_config(64)
+    N, L = [int(v) for v in f["N"]], [float(v) for v in f["L"]]
+    R.set_threads(threads)
+    t0 = time.perf_counter()
+    rp = R.build_problem(N, L, tuple(float(v) for v in f["omegas"]), float(f["g"]), float(f["gdd"]), f["psi"],
+                         float(f["mu"]), V=trap(N, L, tuple(float(v) for v in f["omegas"])), Rc=float(f["rc"]))
+    u = np.random.default_rng(cfg["seed"]).standard_normal((cfg["sizeSub"], int(np.prod(N))))
+    rp.set_solver_params(cfg["nev"], cfg["sizeSub"], 2000, cfg["tol"])
+    rp.set_initial_block(np.concatenate([u, u], axis=1))
+    res = rp.solve(criterion=R.CONV_TRUE_RESIDUAL, deflate=True)
+    rp.close()
+    wall = time.perf_counter() - t0
+    return {"grid": N, "nev": cfg["nev"], "sizeSub": cfg["sizeSub"], "seconds": wall,
+            "iterations": int(res["iterations"]), "converged": int(res["converged"]), "cores": threads,
+            "eigenvalues_head": [float(v) for v in res["eigvals"][:4]],
+            "what": "one whole reference-path solve to tolerance, timed end to end on the host cores"}
+
+
 def project_to_tolerance(tl, first, count, cached):
     """Time to tolerance of the reference path from a live sample: the live
     set-up (t[1] - t[0]) plus the cached full solve's loop time scaled by the
@@ -246,6 +273,8 @@ def run_reference(args, cfg):
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_anchor:
+        line["anchor_64"] = reference_anchor_64(threads)
     print(json.dumps(line))
     return 0
 
@@ -617,6 +646,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-iters", type=int, default=1,
                     help="whole reference-path iterations timed for cpu_baseline")
+    ap.add_argument("--no-anchor", action="store_true",
+                    help="--impl reference: skip the whole 64^3 reference-path solve timed beside the sample")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the mixed-precision variant measured beside the FP64 headline")
     args = ap.parse_args()
