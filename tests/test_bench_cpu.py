@@ -31,3 +31,26 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_projection_and_cache_key():
+    """The reference arm's time to tolerance: live set-up plus the cached
+    solve's loop time scaled by the live/cached ratio of the sampled
+    iterations; the cached solve is used only for the psi0 whose mu it was
+    made from."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    cached = {"timeline": np.array([0.0, 10.0, 12.0, 14.0, 16.0, 18.0]), "iterations": 4}
+    tl = np.array([100.0, 105.0, 106.0, 107.0, 108.0])  # set-up 5 s, iterations of 1 s
+    value, live, n = bench.project_to_tolerance(tl, 1, 2, cached)
+    assert n == 4 and list(live) == [1.0, 1.0]
+    assert abs(value - (5.0 + 8.0 * 0.5)) < 1e-12  # cached loop 8 s at half the cached speed
+    value, live, n = bench.project_to_tolerance(tl, 1, 2, None)
+    assert value is None and n is None
+    c = bench.cached_solve(128)
+    assert c is not None and int(c["iterations"]) > 0
+    assert bench.cached_solve(128, float(c["mu"])) is not None
+    assert bench.cached_solve(128, float(c["mu"]) * (1 + 1e-6)) is None
