@@ -181,3 +181,25 @@ def test_oracle_solve_matches_reference_solve_path():
         r = O.matmulK(oc, Mv) - res["eigvals"][j] ** 2 * v[j]
         assert np.linalg.norm(r) / np.linalg.norm(v[j]) <= tol
     rp.close()
+
+
+def test_reference_solve_path_p_normalisation_option():
+    """The oracle build's iLOBPCG with the projected P SVQB-normalised
+    (normalize_p) and without (the default, as on the GPU): same eigenvalues
+    (1e-12) and iteration counts within one on the 16^3 dipolar problem."""
+    f = np.load(os.path.join(HERE, "golden", "gs16.npz"))
+    N = [int(v) for v in f["N"]]
+    L = [float(v) for v in f["L"]]
+    om = [float(v) for v in f["omegas"]]
+    oc = O.Ctx(3, N, L)
+    X0 = O.gaussian_block_bpositive(oc, 8, 0)
+    out = []
+    for norm in (False, True):
+        rp = R.build_problem(N, L, om, float(f["g"]), float(f["gdd"]), f["psi"], float(f["mu"]), Rc=float(f["rc"]))
+        rp.set_solver_params(4, 8, 400, 1e-8)
+        rp.set_initial_block(X0)
+        out.append(rp.solve(criterion=R.CONV_TRUE_RESIDUAL, deflate=True, normalize_p=norm))
+        rp.close()
+    assert all(r["converged"] >= 4 for r in out)
+    assert np.all(np.abs(out[0]["eigvals"] - out[1]["eigvals"]) / np.abs(out[1]["eigvals"]) < 1e-12)
+    assert abs(int(out[0]["iterations"]) - int(out[1]["iterations"])) <= 1
