@@ -97,17 +97,10 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// the mbarrier gets one arrival once all of this thread's prior cp.async
-// copies have landed (the arrival counts toward the expected count)
-__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
+// one arrival of this thread on the mbarrier (release: its prior writes are
+// visible to the thread that observes the phase)
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-// barrier among the first `nthreads` threads of the CTA (named barrier 1)
-__device__ __forceinline__ void bar_sync_part(int nthreads) {
-  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
 // generic-proxy shared-memory writes become visible to the tensor core
