@@ -329,11 +329,13 @@ __device__ __forceinline__ void oz_unit(const OzArgs &g, int unit, int &tile, in
   }
 }
 
-// C = A^T B over a long row range, A (rows x ka) and B (rows x kb) FP64,
-// column-major, each column scaled by its maximum over all rows (pre-pass).
-// Persistent: one CTA per SM walks the work units (task, 128 x 64 output
-// tile, 16384-row chunk) chunk by chunk, so that the CTAs working at one
-// time share rows in L2.  Warp-specialised per unit:
+// C = A^T B over a long row range, A (rows x ka) and B (rows x kb) FP64 or
+// FP32, column-major, each column scaled by its maximum over all rows
+// (pre-pass).  Persistent: one CTA per SM walks the work units (packed
+// 128 x 64 output tile, 16384-row chunk) chunk by chunk, so that the CTAs
+// working at one time share rows in L2.  A tile's two 64-row halves are
+// 64-column slices of A operands that share the tile's B operand (see
+// OzTile).  Warp-specialised per unit:
 //  * 16 digit warps: each thread loads 8 rows of one A column and 4 rows of
 //    one B column straight into registers two steps ahead, turns them into
 //    digits and stores them into a digit stage (thread-to-column mapping
