@@ -1,5 +1,5 @@
 // bdg_tc.cu -- tensor-core (tcgen05, sm_100a) kernels of the solver's FP64
-// contractions.
+// and FP32 contractions (Gram and basis update through int8 digits).
 //
 // k_tc_i8_gemm: D = A B^T with int8 A (M x K) and B (N x K), K contiguous,
 // int32 D; one 128 x 64 output tile per CTA, K in steps of 32 through a
